@@ -1,0 +1,218 @@
+"""Generate the golden fixtures by running the reference package itself.
+
+Run from the repository root, in a checkout that has the reference project
+next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
+
+    python tests/golden/make_golden.py
+
+Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
+cores as ``<train>_<k>`` arrays plus ``<train>_n``), the call's arguments
+(``args_json``) and the reference's outputs.  The fixtures are read by the
+tests; this script is the only thing that imports the reference, and it is
+never run by the tests.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import sys
+import time
+
+# one BLAS thread: the reference's results are then reproducible run to run
+os.environ["OPENBLAS_NUM_THREADS"] = "1"
+
+import numpy as np  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REFERENCE = os.environ.get("TTNUMPY_REFERENCE", "/root/reference")
+sys.path.insert(0, REFERENCE)
+sys.path.insert(0, ROOT)
+
+import ttnumpy as tt  # noqa: E402
+from ttnumpy.solvers.common import relative_residual  # noqa: E402
+
+from ttnumpy_b200 import problems as P  # noqa: E402
+
+
+def pack(out: dict, name: str, train) -> None:
+    cores = train.cores if hasattr(train, "cores") else train
+    out[f"{name}_n"] = np.array(len(cores))
+    for k, c in enumerate(cores):
+        out[f"{name}_{k}"] = np.asarray(c, dtype=np.float64)
+    oc = getattr(train, "orth_center", None)
+    out[f"{name}_oc"] = np.array(-1 if oc is None else oc)
+
+
+def ref_train(cores, orth_center=None):
+    t = tt.TensorTrain([np.array(c, dtype=np.float64) for c in cores])
+    t.orth_center = orth_center
+    return t
+
+
+def save(name: str, data: dict, args: dict) -> None:
+    data["args_json"] = np.array(json.dumps(args))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+    size = os.path.getsize(os.path.join(HERE, f"{name}.npz"))
+    print(f"{name}: {size / 1024:.1f} KiB")
+
+
+def amen_case(name, A, b, x0=None, full=True, **kw):
+    """Run the reference amen and store inputs plus outputs."""
+    data = {}
+    pack(data, "A", A)
+    pack(data, "b", b)
+    if x0 is not None:
+        pack(data, "x0", x0)
+    t0 = time.perf_counter()
+    x, info = tt.amen(A, b, x0=x0, return_info=True, **kw)
+    elapsed = time.perf_counter() - t0
+    pack(data, "x", x)
+    data["residuals"] = np.array(info.residuals, dtype=np.float64)
+    data["max_bonds"] = np.array(info.max_bonds)
+    data["bonds"] = np.array(x.bonds)
+    data["num_sweeps_run"] = np.array(info.num_sweeps_run)
+    data["stop_reason"] = np.array(str(info.stop_reason))
+    data["local_solves"] = np.array(info.local_solves)
+    data["local_inexact"] = np.array(info.local_inexact)
+    data["final_residual"] = np.array(relative_residual(A, b, x))
+    data["x_norm"] = np.array(x.tt_norm())
+    if full:
+        data["x_full"] = np.asarray(x.get_full_tensor(), dtype=np.float64).reshape(-1)
+    data["seconds"] = np.array(elapsed)
+    save(name, data, kw)
+
+
+def qtt_laplacian_1d(order):
+    """The reference test operator: TT-SVD (error 0) of the 1-D Dirichlet
+    Laplacian with diagonal -2, as its solver test helper builds it."""
+    size = 2**order
+    h = 1.0 / (size + 1)
+    lap = (np.diag(-2.0 * np.ones(size)) + np.diag(np.ones(size - 1), 1)
+           + np.diag(np.ones(size - 1), -1)) / h**2
+    A = tt.tt_svd(lap.reshape([2] * 2 * order), physical_indexes=[(2, 2)] * order,
+                  ttm=True, error=0)
+    return A, lap
+
+
+def main() -> None:
+    meta = {"reference_version": tt.__version__, "numpy": np.__version__}
+    import scipy
+    meta["scipy"] = scipy.__version__
+
+    # --- AMEn, reference test cases -------------------------------------
+    A, _ = qtt_laplacian_1d(6)
+    b = tt.ones([2] * 6)
+    x0 = tt.ones([2] * 6, ranks=1).orthonormalize(canonical="right")
+    amen_case("amen_qtt_lap1d_o6", A, b, x0, kickrank=3, error_threshold=1e-12,
+              residual_tol=1e-8, max_sweeps=20, symmetric=True, seed=0)
+
+    rng = np.random.default_rng(5)
+    mat = np.eye(32) + 0.3 * rng.random((32, 32))
+    A = tt.tt_svd(mat.reshape([2] * 10), physical_indexes=[(2, 2)] * 5, ttm=True, error=0)
+    vec = rng.random(32)
+    b = tt.tt_svd(vec.reshape([2] * 5), error=0)
+    amen_case("amen_nonsym_o5", A, b, kickrank=4, error_threshold=1e-12,
+              residual_tol=1e-9, max_sweeps=25, seed=3)
+
+    # same system, local solves forced onto GMRES
+    amen_case("amen_nonsym_gmres", A, b, kickrank=4, error_threshold=1e-12,
+              residual_tol=1e-9, max_sweeps=25, seed=3, direct_solve_size=4)
+
+    # small Laplacian, MINRES local solves (direct_solve_size lowered)
+    A = ref_train(P.laplacian_nd(4, 8))
+    b = tt.rand([8] * 4, ranks=2, seed=0)
+    amen_case("amen_lap4_minres", A, b, residual_tol=1e-8, symmetric=True,
+              max_sweeps=20, seed=0, direct_solve_size=20)
+
+    # threshold truncation mode, no residual target, with max_rank cap
+    A = ref_train(P.laplacian_nd(5, 6))
+    b = tt.rand([6] * 5, ranks=3, seed=1)
+    amen_case("amen_lap5_threshold", A, b, error_threshold=1e-10, max_sweeps=4,
+              symmetric=True, seed=2, max_rank=7)
+
+    # config 1 as written: one sweep (max_sweeps default 1)
+    A = ref_train(P.laplacian_nd(8, 32))
+    b = tt.rand([32] * 8, ranks=4, seed=0)
+    amen_case("amen_cfg1_literal", A, b, full=False, residual_tol=1e-8, symmetric=True)
+
+    # config 3: QTT 2-D Poisson on 2^10 x 2^10, as solve_poisson_tt calls it
+    p = P.qtt_poisson_2d(10)
+    A = ref_train(p.A)
+    b = ref_train(p.b)
+    amen_case("amen_cfg3", A, b, full=False, residual_tol=1e-8, symmetric=True,
+              max_sweeps=20, seed=0)
+
+    # two parametric diffusion draws (config 4 family), small enough to be quick
+    for i, (d, n, seed) in enumerate([(4, 16, 11), (5, 16, 12)]):
+        theta = np.random.default_rng(seed).uniform(-1, 1, size=d)
+        p = P.parametric_diffusion(d, n, theta)
+        amen_case(f"amen_diffusion_{i}", ref_train(p.A), ref_train(p.b), full=False,
+                  residual_tol=1e-8, symmetric=True, max_sweeps=20, seed=0)
+
+    # --- TT rounding (config 2 family) -----------------------------------
+    for name, d, n, r, err, mr, gauss in [
+        ("truncate_pair_u", 8, 4, 8, 1e-6, None, False),
+        ("truncate_pair_g", 8, 4, 8, 1e-6, None, True),
+        ("truncate_pair_maxrank", 8, 4, 8, 1e-6, 5, True),
+        ("truncate_pair_d16", 16, 4, 32, 1e-6, None, False),
+    ]:
+        data = {}
+        outs = []
+        for pair in range(1 if d == 16 else 3):
+            if gauss:
+                g = np.random.default_rng(pair)
+                ranks = [1] + [r] * (d - 1) + [1]
+                p = tt.TensorTrain([g.standard_normal((ranks[k], n, 1, ranks[k + 1])) for k in range(d)])
+                q = tt.TensorTrain([g.standard_normal((ranks[k], n, 1, ranks[k + 1])) for k in range(d)])
+            else:
+                p = tt.rand([n] * d, ranks=r, seed=2 * pair)
+                q = tt.rand([n] * d, ranks=r, seed=2 * pair + 1)
+            if gauss:
+                # uniform inputs are regenerated from their seeds by the tests
+                pack(data, f"p{pair}", p)
+                pack(data, f"q{pair}", q)
+            s = p + q
+            out = s.truncate(error=err, max_rank=mr)
+            pack(data, f"out{pair}", out)
+            data[f"bonds{pair}"] = np.array(out.bonds)
+            data[f"err{pair}"] = np.array((out - s).tt_norm() / s.tt_norm())
+            outs.append(out)
+        save(name, data, {"error": err, "max_rank": mr, "gaussian": gauss})
+
+    # truncate with an orthogonality centre in the left half, canonical="left"
+    data = {}
+    t = tt.rand([3] * 7, ranks=6, seed=9)
+    t.orthonormalize("left", center_position=2, inplace=True)
+    pack(data, "t", t)
+    for canon in ("auto", "left", "right"):
+        out = t.truncate(error=1e-3, canonical=canon)
+        pack(data, f"out_{canon}", out)
+    save("truncate_canonical", data, {"error": 1e-3})
+
+    # --- TTM by TT products and relative residuals ------------------------
+    data = {}
+    g = np.random.default_rng(7)
+    modes = [3, 4, 2, 5]
+    rA = [1, 2, 3, 2, 1]
+    rx = [1, 3, 2, 4, 1]
+    A = tt.TensorTrain([g.standard_normal((rA[k], modes[k], modes[k], rA[k + 1])) for k in range(4)])
+    x = tt.TensorTrain([g.standard_normal((rx[k], modes[k], 1, rx[k + 1])) for k in range(4)])
+    b = tt.rand(modes, ranks=2, seed=3)
+    y = A.dot(x)
+    pack(data, "A", A)
+    pack(data, "x", x)
+    pack(data, "b", b)
+    pack(data, "y", y)
+    data["y_full"] = np.asarray(y.get_full_tensor(), dtype=np.float64).reshape(-1)
+    data["residual"] = np.array(relative_residual(A, b, x))
+    data["b_norm"] = np.array(b.tt_norm())
+    save("dot_residual", data, {})
+
+    with open(os.path.join(HERE, "meta.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()
