@@ -1,0 +1,361 @@
+/*
+ * libttb200: B200 (sm_100a) kernels for the tensor-train solve path.
+ *
+ * C ABI.  Every pointer argument named in a problem struct is a device
+ * pointer (float64 unless stated), every size is in elements, every stride
+ * is an element stride, and dense arrays are row major unless the field
+ * says otherwise.  Problem structs are passed as host arrays; one call
+ * processes ``count`` independent problems in grouped launches.  Calls are
+ * asynchronous on ``stream`` (a cudaStream_t; NULL is the legacy default
+ * stream) unless stated, and return 0 or a cudaError_t code.  No entry point
+ * allocates device memory: work areas are passed in, sized by the
+ * ttb_*_work_doubles functions.
+ *
+ * Index conventions follow the reference (ttnumpy 0.3.0,
+ * ttnumpy/tensor_train.py:150-244): cores are (r, row_mode, col_mode, r'),
+ * environments with an operator are indexed (target, operator, frame),
+ * without one (target, frame) (ttnumpy/solvers/common.py:149-217).
+ */
+#ifndef TTB200_H
+#define TTB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Version of the library ABI (incremented on incompatible changes). */
+int ttb_version(void);
+
+/* Number of the library's own kernels launched since load (all devices). */
+long long ttb_launch_count(void);
+
+/* ------------------------------------------------------------------------
+ * Dense float64 GEMM on strided batched views:
+ *   C[b] = alpha * A[b] * B[b] + beta * C[b],  b = 0..batch-1
+ * with A[b](i, k) = a[b*a_bs + i*a_rs + k*a_cs] and likewise for B and C
+ * (a stride of 0 shares an operand across the batch; beta == 0 never reads
+ * C).  This is the contraction engine under every tensordot/einsum of the
+ * reference path (e.g. ttnumpy/utils.py:72-83 _multiply_left/_right).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* a;
+  const double* b;
+  double* c;
+  int m, n, k, batch;
+  long long a_rs, a_cs, a_bs;
+  long long b_rs, b_cs, b_bs;
+  long long c_rs, c_cs, c_bs;
+  double alpha, beta;
+} ttb_gemm_t;
+int ttb_gemm(const ttb_gemm_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Environment update: one step of the left or right projection recursion,
+ * replacing prepare_left_environment / prepare_right_environment
+ * (ttnumpy/solvers/common.py:149-188, 191-217).
+ *   left  (side 0): env (t, R, f) or (t, f); frame core (f, n, f2);
+ *                   op (R, n, m, R2) or NULL; target (t, m, t2);
+ *                   out (t2, R2, f2) or (t2, f2)
+ *   right (side 1): env (t, R, f) or (t, f); frame core (f2, n, f);
+ *                   op (R2, n, m, R) or NULL; target (t2, m, t);
+ *                   out (t2, R2, f2) or (t2, f2)
+ * Without an operator set R = R2 = 1 and n = m.  ``work`` holds
+ * ttb_env_work_doubles() doubles.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* env;
+  const double* frame;
+  const double* op;
+  const double* target;
+  double* out;
+  double* work;
+  int side;
+  int f, f2, t, t2, R, R2, n, m;
+} ttb_env_t;
+long long ttb_env_work_doubles(const ttb_env_t* problem);
+int ttb_env_update(const ttb_env_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * One-site local operator applied to ``cols`` vectors (matrix-free matvec /
+ * matmat), replacing local_operator_one_site (ttnumpy/solvers/one_site.py:
+ * 78-115), and, with a rectangular frame, the A x part of residual_core
+ * (ttnumpy/solvers/amen.py:142-158):
+ *   y[c, j, k, q] = alpha * sum L[i, a, j] A[a, k, l, b] Rt[p, b, q] x[c, i, l, p]
+ *                   + beta * y[c, j, k, q]
+ * left (lt, R, lf), op (R, n, m, R2), right (rt, R2, rf), x cols x (lt, m, rt),
+ * y cols x (lf, n, rf).  ``work`` holds ttb_local_work_doubles() doubles.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* left;
+  const double* op;
+  const double* right;
+  const double* x;
+  double* y;
+  double* work;
+  int lt, lf, R, R2, n, m, rt, rf, cols;
+  double alpha, beta;
+} ttb_local_t;
+long long ttb_local_work_doubles(const ttb_local_t* problem);
+int ttb_local_apply(const ttb_local_t* problems, int count, void* stream);
+
+/* Explicit one-site local matrix, replacing local_explicit_matrix_one_site
+ * (ttnumpy/solvers/one_site.py:49-75).  Output is column major with
+ * leading dimension rows = lf*n*rf: out[row + col*rows], rows indexed
+ * (lf, n, rf), columns (lt, m, rt). */
+typedef struct {
+  const double* left;
+  const double* op;
+  const double* right;
+  double* out;
+  int lt, lf, R, R2, n, m, rt, rf;
+} ttb_local_matrix_t;
+int ttb_local_matrix(const ttb_local_matrix_t* problems, int count, void* stream);
+
+/* One-site right-hand side / projection of a TT core, replacing
+ * local_rhs_one_site (ttnumpy/solvers/one_site.py:27-46):
+ *   out[i, j, l] = alpha * sum_{a,c} Lb[a, i] core[a, j, c] Rb[c, l] + beta * out
+ * left (a, i), core (a, n, c), right (c, l), out (i, n, l).
+ * ``work`` holds a*n*l doubles. */
+typedef struct {
+  const double* left;
+  const double* core;
+  const double* right;
+  double* out;
+  double* work;
+  int a, i, n, c, l;
+  double alpha, beta;
+} ttb_project_t;
+int ttb_project(const ttb_project_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Economic Householder QR of an m x k strided matrix: Q (m x p), R (p x k),
+ * p = min(m, k), as scipy.linalg.qr(mode="economic") is used by
+ * left_orthonormalize / right_orthonormalize (ttnumpy/utils.py:86-136) and
+ * _shift_center_right / _shift_center_left
+ * (ttnumpy/solvers/one_site.py:181-209).  q or r may be NULL.  ``work``
+ * holds ttb_qr_work_doubles(m, k) doubles (used when the factorisation does
+ * not fit in shared memory).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* a;
+  long long a_rs, a_cs;
+  double* q;
+  long long q_rs, q_cs;
+  double* r;
+  long long r_rs, r_cs;
+  double* work;
+  int m, k;
+} ttb_qr_t;
+long long ttb_qr_work_doubles(int m, int k);
+int ttb_qr(const ttb_qr_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Thin SVD of an m x k strided matrix, a = u diag(s) vh with s descending,
+ * p = min(m, k): u (m x p), s (p), vh (p x k).  Householder QR followed by
+ * one-sided Jacobi on the triangular factor.  Replaces the LAPACK gesdd /
+ * gesvd calls of left_svd / right_svd (ttnumpy/utils.py:336-460) and of
+ * _truncate_core_right / _left (ttnumpy/solvers/amen.py:254-260, 301-307).
+ * ``status`` (device int, may be NULL) receives the Jacobi sweeps used or
+ * -1 when the sweep cap was reached.  ``work`` holds
+ * ttb_svd_work_doubles(m, k) doubles.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* a;
+  long long a_rs, a_cs;
+  double* u;
+  long long u_rs, u_cs;
+  double* s;
+  double* vh;
+  long long vh_rs, vh_cs;
+  double* work;
+  int* status;
+  int m, k;
+} ttb_svd_t;
+long long ttb_svd_work_doubles(int m, int k);
+int ttb_svd(const ttb_svd_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Dense solve a x = b by Gaussian elimination with partial pivoting,
+ * replacing scipy.linalg.solve in _solve_local_system
+ * (ttnumpy/solvers/common.py:766-774).  a is n x n column major with
+ * leading dimension lda and is overwritten; b (n) is overwritten with x.
+ * ``info`` (device int, may be NULL) receives 0 or the 1-based index of a
+ * zero pivot.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  double* a;
+  long long lda;
+  double* b;
+  int* info;
+  int n;
+} ttb_lu_t;
+int ttb_lu_solve(const ttb_lu_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Strided 4-D copy dst = alpha * scale[i_axis] * src (src NULL: the value
+ * without the src factor; scale NULL: no per-index factor), the core
+ * concatenations, zero padding and diagonal scalings of the reference
+ * (ttnumpy/tensor_train.py:254-322 add, ttnumpy/solvers/amen.py:275, 322,
+ * 325-392 truncation carries and enrichment).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* src;
+  double* dst;
+  const double* scale;
+  int d0, d1, d2, d3;
+  long long s0, s1, s2, s3;
+  long long t0, t1, t2, t3;
+  double alpha;
+  int scale_axis;
+} ttb_copy_t;
+int ttb_copy(const ttb_copy_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * TTM-by-TT core product, replacing the einsum of TensorTrain.dot
+ * (ttnumpy/tensor_train.py:483-495):
+ *   out[(a, x), i, k, (b, y)] = sum_j op[a, i, j, b] * core[x, j, k, y]
+ * op (ra, n, m, ra2), core (rx, m, kk, rx2), out (ra*rx, n, kk, ra2*rx2).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* op;
+  const double* core;
+  double* out;
+  int ra, ra2, n, m, rx, rx2, kk;
+} ttb_kron_t;
+int ttb_kron(const ttb_kron_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Sums of squares and norms.  out[p] = sqrt(sum of squares of x[0..n-1])
+ * (the np.linalg.norm calls of the reference, e.g.
+ * ttnumpy/tensor_train.py:529-538, ttnumpy/solvers/common.py:776,787),
+ * with an optional y: out = ||x - y||.  Deterministic order.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* x;
+  const double* y;
+  double* out;
+  long long n;
+} ttb_norm_t;
+int ttb_norm(const ttb_norm_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Residual-budget truncation rank, replacing _truncation_rank_by_residual
+ * (ttnumpy/solvers/common.py:812-866).  contrib holds ``limit`` rows of
+ * length n (row r = A_loc applied to the r-th rank-one term of the SVD);
+ * b is b_loc.  rank[0] receives the smallest r + 1 with
+ * ||-b + sum_{i<=r} contrib_i|| <= max(damp * exact[0], 0.5 * tol * ||b||),
+ * or ``limit`` when no prefix meets it (capped[0] = 1 then if limit < p).
+ * s0 is the largest singular value; s0 == 0 gives rank 1.  work holds
+ * ttb_rank_work_doubles(n, limit) doubles.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* contrib;
+  const double* b;
+  const double* exact;
+  const double* s;
+  int* rank;
+  double* work;
+  long long n;
+  int limit, p;
+  double damp, tol;
+} ttb_rank_t;
+long long ttb_rank_work_doubles(long long n, int limit);
+int ttb_rank_residual(const ttb_rank_t* problems, int count, void* stream);
+
+/* Threshold rank rules on descending singular values s (p of them):
+ * mode 0: _svd_truncation_rank (ttnumpy/solvers/common.py:872-885),
+ *         count of s / s[0] > value, floored at 1, capped at max_rank;
+ * mode 1: truncated_bond (ttnumpy/utils.py:22-69), smallest r whose tail
+ *         norm is <= value after the eps * p * s[0] noise floor, floored
+ *         at 1, capped at max_rank.
+ * max_rank <= 0 means no cap. */
+typedef struct {
+  const double* s;
+  int* rank;
+  int p, mode, max_rank;
+  double value;
+} ttb_rank_rule_t;
+int ttb_rank_threshold(const ttb_rank_rule_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * MINRES on the one-site local operator, replacing scipy.sparse.linalg
+ * .minres as _solve_local_system calls it (ttnumpy/solvers/common.py:
+ * 783-784; SciPy 1.18.1, the Paige-Saunders algorithm with SciPy's
+ * stopping rules).  Solves op x = b from the initial guess in x (zero
+ * when ``warm`` is 0), relative tolerance rtol, at most maxiter
+ * iterations (<= 0 means 5 n).  The call blocks the host until every
+ * problem stopped: it launches the iterations and reads the stop flags
+ * back every few iterations.  istop[0] receives SciPy's istop code and
+ * iters[0] the iterations run (both device ints).  work holds
+ * ttb_minres_work_doubles() doubles; ``flags`` is a device array of
+ * ``count`` ints the solver uses to report which problems stopped.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  ttb_local_t op;  /* x, y, alpha, beta, cols are set by the solver */
+  const double* b;
+  double* x;
+  double* work;
+  int* istop;
+  int* iters;
+  long long n;
+  double rtol;
+  int maxiter;
+  int warm;
+} ttb_krylov_t;
+long long ttb_minres_work_doubles(const ttb_krylov_t* problem);
+int ttb_minres(const ttb_krylov_t* problems, int count, int* flags, void* stream);
+
+/* GMRES(restart) with SciPy 1.18.1's gmres semantics (modified
+ * Gram-Schmidt Arnoldi, Givens rotations, atol = rtol * ||b||, restart 20,
+ * maxiter outer cycles, <= 0 meaning 10 n), replacing
+ * scipy.sparse.linalg.gmres in _solve_local_system
+ * (ttnumpy/solvers/common.py:785-786).  Same calling convention as
+ * ttb_minres; istop receives 0 on convergence, 1 otherwise. */
+long long ttb_gmres_work_doubles(const ttb_krylov_t* problem, int restart);
+int ttb_gmres(const ttb_krylov_t* problems, int count, int restart, int* flags, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Batched TT rounding of sums of two trains, one thread block per pair,
+ * replacing (p + q).truncate(error, max_rank) with method="direct"
+ * (ttnumpy/tensor_train.py:254-322, 852-940; ttnumpy/utils.py:86-136,
+ * 364-460): left QR sweep of the block-diagonal sum, then right SVD sweep
+ * with the tail-norm rule.  All trains of a batch share d and the mode
+ * sizes; p, q are packed core by core (core k of pair i at
+ * p + i*p_stride + p_off[k]), likewise q.  The rounded cores are written to
+ * out (pair i at out + i*out_stride, core k at offset out_off[i*d + k] of
+ * that block, computed on the device) and the bonds to bonds[i*(d+1)..].
+ * Requires every bond of p + q to be <= 64 and mode * bond <= 256 on both
+ * sides of every core (status[i] = -2 otherwise; -1 when a Jacobi sweep
+ * cap was reached).  Core k of the result is stored at slot k of
+ * TTB_ROUND_SLOT doubles (out_stride >= d * TTB_ROUND_SLOT).  work holds
+ * ttb_round_work_doubles() doubles per pair (work_stride).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* p;
+  const double* q;
+  const long long* p_off;   /* device, d entries */
+  const long long* q_off;   /* device, d entries */
+  const int* p_bonds;       /* device, d + 1 entries */
+  const int* q_bonds;       /* device, d + 1 entries */
+  const int* modes;         /* device, d entries */
+  long long p_stride, q_stride;
+  double* out;
+  long long out_stride;
+  long long* out_off;       /* device, pairs * d entries (written) */
+  int* bonds;               /* device, pairs * (d + 1) entries (written) */
+  double* work;
+  long long work_stride;
+  int* status;              /* device, pairs entries (written) */
+  int pairs, d;
+  double error;
+  int max_rank;
+} ttb_round_t;
+#define TTB_ROUND_SLOT 16384
+long long ttb_round_work_doubles(int d, int max_mode, int max_bond);
+int ttb_round_batch(const ttb_round_t* problem, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TTB200_H */

@@ -1,0 +1,144 @@
+"""GPU AMEn against the reference's own results (golden fixtures) and the
+oracle.
+
+Comparisons are on what the algorithm promises, not on raw cores (QR/SVD
+signs are ambiguous and the enrichment is chaotic in rounding): the stop
+reason, the final relative residual recomputed on the host by the oracle
+(must meet ``residual_tol``), and the distance between the GPU solution and
+the reference solution, ``||x - x_ref|| / ||x_ref||``, which for a converged
+solve is bounded by the conditioning times the tolerance (1e-6 here, 1e-8 on
+the reference test that checks against a dense solve).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_train, load_golden
+from oracle import tt_oracle as O
+from ttnumpy_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def tt():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import ttnumpy_b200
+
+    return ttnumpy_b200
+
+
+def otrain(t):
+    return O.Train(t.to_numpy(), t.orth_center)
+
+
+def rel_tt(a: O.Train, b: O.Train) -> float:
+    return O.tt_norm(O.add(a, O.scale(b, -1.0))) / O.tt_norm(b)
+
+
+CONVERGED = ["amen_qtt_lap1d_o6", "amen_nonsym_o5", "amen_nonsym_gmres", "amen_lap4_minres",
+             "amen_cfg3", "amen_diffusion_0", "amen_diffusion_1"]
+
+
+@pytest.mark.parametrize("case", CONVERGED)
+def test_amen_converged_cases(tt, case):
+    data = load_golden(case)
+    A_c, _ = golden_train(data, "A")
+    b_c, b_oc = golden_train(data, "b")
+    A, b = tt.TensorTrain(A_c), tt.TensorTrain(b_c, orth_center=b_oc)
+    x0 = None
+    if "x0_n" in data:
+        c, oc = golden_train(data, "x0")
+        x0 = tt.TensorTrain(c, orth_center=oc)
+    args = dict(data["args"])
+    x, info = tt.amen(A, b, x0=x0, return_info=True, **args)
+    assert str(data["stop_reason"]) == "converged"
+    assert info.converged, (case, info)
+    tol = args["residual_tol"]
+    host_res = O.relative_residual(O.Train(A_c), O.Train(b_c, b_oc), otrain(x))
+    assert host_res <= tol * 1.05, host_res
+    assert info.residuals[-1] == pytest.approx(host_res, rel=1e-6, abs=1e-3 * tol)
+    assert len(info.max_bonds) == info.num_sweeps_run
+    assert x.orth_center == 0
+    ref = O.Train(golden_train(data, "x")[0])
+    assert rel_tt(otrain(x), ref) < 1e-6
+    # sweeps within one of the reference's count
+    assert abs(info.num_sweeps_run - int(data["num_sweeps_run"])) <= 1
+
+
+def test_amen_dense_solution_qtt_laplacian(tt):
+    """The reference test's dense check: solution vs np.linalg.solve < 1e-8
+    (``tests/test_amen.py:257-299``)."""
+    data = load_golden("amen_qtt_lap1d_o6")
+    A_c, _ = golden_train(data, "A")
+    x0c, x0oc = golden_train(data, "x0")
+    A = tt.TensorTrain(A_c)
+    b = tt.TensorTrain(golden_train(data, "b")[0])
+    x, info = tt.amen(A, b, x0=tt.TensorTrain(x0c, orth_center=x0oc), return_info=True,
+                      **data["args"])
+    dense = O.Train(A_c).full()
+    exact = np.linalg.solve(dense, np.ones(dense.shape[0]))
+    got = x.get_full_tensor().reshape(-1)
+    assert info.converged
+    assert np.linalg.norm(got - exact) / np.linalg.norm(exact) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["amen_cfg1_literal", "amen_lap5_threshold"])
+def test_amen_unconverged_cases(tt, case):
+    """Runs that stop on max_sweeps / stagnation: same stop reason, sweeps
+    and rank trace; residual of the same size."""
+    data = load_golden(case)
+    A_c, _ = golden_train(data, "A")
+    b_c, b_oc = golden_train(data, "b")
+    x, info = tt.amen(tt.TensorTrain(A_c), tt.TensorTrain(b_c, orth_center=b_oc),
+                      return_info=True, **data["args"])
+    assert str(info.stop_reason) == str(data["stop_reason"])
+    assert info.num_sweeps_run == int(data["num_sweeps_run"])
+    ref = np.asarray(data["residuals"])
+    got = np.asarray(info.residuals)
+    assert got.shape == ref.shape
+    assert np.all(got <= 2.0 * ref) and np.all(got >= 0.5 * ref), (got, ref)
+    assert max(x.bonds) <= max(int(v) for v in data["max_bonds"]) + 8
+
+
+def test_amen_deterministic(tt):
+    """Equal seeds give bit-identical results (``tests/test_amen.py:480-492``)."""
+    A_c = P.laplacian_nd(4, 8)
+    b_c = P.random_tt([8] * 4, 2, seed=4)
+    outs = []
+    for _ in range(2):
+        x = tt.amen(tt.TensorTrain(A_c), tt.TensorTrain(b_c), residual_tol=1e-8, symmetric=True,
+                    max_sweeps=6, seed=7, direct_solve_size=30)
+        outs.append(x.to_numpy())
+    assert all(np.array_equal(a, b) for a, b in zip(*outs))
+
+
+def test_amen_validation_errors(tt):
+    A = tt.TensorTrain(P.laplacian_nd(3, 4))
+    b = tt.TensorTrain(P.random_tt([4] * 3, 2, seed=0))
+    with pytest.raises(ValueError):
+        tt.amen(A, b, kickrank=0)
+    with pytest.raises(ValueError):
+        tt.amen(A, b, max_rank=0)
+    with pytest.raises(ValueError):
+        tt.amen(A, b, residual_damp=0.5)
+    with pytest.raises(ValueError):
+        tt.amen(A, b, local_solver="cholesky")
+    with pytest.raises(tt.WrongTTType):
+        tt.amen(b, b)
+    with pytest.raises(tt.DimensionMismatch):
+        tt.amen(A, tt.TensorTrain(P.random_tt([4] * 4, 2, seed=0)))
+
+
+def test_amen_config1_converges(tt):
+    """The 8-D Laplacian (32 points per axis) with a rank-4 right-hand side
+    reaches 1e-8, checked by the host oracle."""
+    A_c = P.laplacian_nd(8, 32)
+    b_c = P.random_tt([32] * 8, 4, seed=0)
+    x, info = tt.amen(tt.TensorTrain(A_c), tt.TensorTrain(b_c), residual_tol=1e-8,
+                      symmetric=True, max_sweeps=20, seed=0, return_info=True)
+    assert info.converged, info
+    host_res = O.relative_residual(O.Train(A_c), O.Train(b_c), otrain(x))
+    assert host_res <= 1.05e-8

@@ -1,0 +1,145 @@
+"""Device TensorTrain (truncate, dot, add, norms, canonical forms) and the
+batched rounding kernel against the golden fixtures and the oracle.
+
+Rounded trains are compared as reconstructions (SVD/QR signs are
+ambiguous): relative difference below 1e-12 for exact operations, below the
+requested truncation error for rounding, and identical bonds.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_train, load_golden
+from oracle import tt_oracle as O
+from ttnumpy_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def tt():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import ttnumpy_b200
+
+    return ttnumpy_b200
+
+
+def otrain(t):
+    return O.Train(t.to_numpy(), t.orth_center)
+
+
+def rel_tt(a: O.Train, b: O.Train) -> float:
+    return O.tt_norm(O.add(a, O.scale(b, -1.0))) / O.tt_norm(b)
+
+
+@pytest.mark.parametrize("case", ["truncate_pair_u", "truncate_pair_g", "truncate_pair_maxrank",
+                                  "truncate_pair_d16"])
+def test_truncate_matches_reference(tt, case):
+    data = load_golden(case)
+    args = data["args"]
+    pairs = 1 if case.endswith("d16") else 3
+    d, r = (16, 32) if case.endswith("d16") else (8, 8)
+    for pair in range(pairs):
+        if args["gaussian"]:
+            p, _ = golden_train(data, f"p{pair}")
+            q, _ = golden_train(data, f"q{pair}")
+        else:
+            p, q = P.random_tt([4] * d, r, 2 * pair), P.random_tt([4] * d, r, 2 * pair + 1)
+        s = tt.TensorTrain(p) + tt.TensorTrain(q)
+        out = s.truncate(error=args["error"], max_rank=args["max_rank"])
+        ref_cores, _ = golden_train(data, f"out{pair}")
+        assert out.bonds == [c.shape[0] for c in ref_cores] + [1]
+        ref = O.Train(ref_cores)
+        assert rel_tt(otrain(out), ref) < 1e-10
+        # rounding error against the untruncated sum is within the request
+        # (a max_rank cap may exceed it, as in the reference)
+        if args["max_rank"] is None:
+            err = rel_tt(otrain(out), O.add(O.Train(p), O.Train(q)))
+            assert err <= args["error"] * 1.0001 + 1e-14
+
+
+def test_truncate_canonical_and_centres(tt):
+    data = load_golden("truncate_canonical")
+    cores, oc = golden_train(data, "t")
+    t = tt.TensorTrain(cores, orth_center=oc)
+    for canon in ("auto", "left", "right"):
+        out = t.truncate(error=1e-3, canonical=canon)
+        ref_cores, ref_oc = golden_train(data, f"out_{canon}")
+        assert out.bonds == [c.shape[0] for c in ref_cores] + [1]
+        assert out.orth_center == ref_oc
+        np.testing.assert_allclose(out.get_full_tensor(), O.Train(ref_cores).full().reshape(
+            out.get_full_tensor().shape), atol=1e-11)
+
+
+def test_dot_norm_residual(tt):
+    data = load_golden("dot_residual")
+    A = tt.TensorTrain(golden_train(data, "A")[0])
+    x = tt.TensorTrain(golden_train(data, "x")[0])
+    b = tt.TensorTrain(golden_train(data, "b")[0])
+    y = A.dot(x)
+    assert y.bonds == list(O.Train(golden_train(data, "y")[0]).bonds)
+    np.testing.assert_allclose(y.get_full_tensor().reshape(-1), data["y_full"], rtol=1e-12,
+                               atol=1e-12)
+    assert (A @ x).bonds == y.bonds
+    assert tt.relative_residual(A, b, x) == pytest.approx(float(data["residual"]), rel=1e-11)
+    assert b.tt_norm() == pytest.approx(float(data["b_norm"]), rel=1e-13)
+
+
+def test_orthonormalize_and_errors(tt):
+    rng = np.random.default_rng(3)
+    cores = [rng.standard_normal(s) for s in [(1, 3, 1, 4), (4, 3, 1, 5), (5, 3, 1, 1)]]
+    t = tt.TensorTrain(cores)
+    full = t.get_full_tensor()
+    left = t.orthonormalize("left")
+    assert left.orth_center == 2
+    np.testing.assert_allclose(left.get_full_tensor(), full, atol=1e-12)
+    c0 = left.cores[0].cpu().numpy().reshape(-1, left.bonds[1])
+    np.testing.assert_allclose(c0.T @ c0, np.eye(c0.shape[1]), atol=1e-13)
+    right = t.orthonormalize("right")
+    assert right.orth_center == 0
+    assert right.tt_norm() == pytest.approx(np.linalg.norm(full), rel=1e-13)
+    assert t.tt_norm() == pytest.approx(np.linalg.norm(full), rel=1e-13)
+    with pytest.raises(tt.DimensionMismatch):
+        t + tt.TensorTrain([rng.standard_normal(s) for s in [(1, 2, 1, 1), (1, 3, 1, 1),
+                                                             (1, 3, 1, 1)]])
+    with pytest.raises(tt.WrongTTFormat):
+        tt.TensorTrain([rng.standard_normal((2, 3, 1, 1)), rng.standard_normal((1, 3, 1, 1))])
+    with pytest.raises(TypeError):
+        t.dot(3)
+    with pytest.raises(ValueError):
+        t.truncate(canonical="mix")
+    with pytest.raises(tt.DimensionMismatch):
+        t.dot(t)
+    with pytest.raises(ValueError):
+        tt.eye([3, 3, 3]).dot(t, error=1e-3)
+
+
+@pytest.mark.parametrize("d,n,r,err,mr,gauss", [(6, 4, 6, 1e-6, None, False),
+                                               (8, 4, 8, 1e-6, None, True),
+                                               (8, 4, 8, 1e-4, 5, True),
+                                               (16, 4, 32, 1e-6, None, False),
+                                               (7, 2, 20, 1e-8, None, True)])
+def test_round_batch_matches_oracle(tt, d, n, r, err, mr, gauss):
+    from ttnumpy_b200.rounding import PackedTrains, round_sum_batch
+
+    pairs = 5
+    rng = np.random.default_rng(d * 100 + r)
+    ranks = [1] + [r] * (d - 1) + [1]
+    if gauss:
+        ps = [[rng.standard_normal((ranks[k], n, 1, ranks[k + 1])) for k in range(d)]
+              for _ in range(pairs)]
+        qs = [[rng.standard_normal((ranks[k], n, 1, ranks[k + 1])) for k in range(d)]
+              for _ in range(pairs)]
+    else:
+        ps = [P.random_tt([n] * d, r, 2 * i) for i in range(pairs)]
+        qs = [P.random_tt([n] * d, r, 2 * i + 1) for i in range(pairs)]
+    res = round_sum_batch(PackedTrains.from_numpy(ps), PackedTrains.from_numpy(qs), err, mr)
+    assert (res.status.cpu().numpy() >= 0).all()
+    for i in range(pairs):
+        s = O.add(O.Train(ps[i]), O.Train(qs[i]))
+        want = O.truncate(s, err, mr)
+        got = otrain(res.train(i))
+        assert got.bonds == want.bonds
+        assert rel_tt(got, want) < max(1e-10, 0.01 * err)

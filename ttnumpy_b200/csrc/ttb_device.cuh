@@ -1,0 +1,497 @@
+// CTA-level float64 building blocks shared by every kernel of libttb200.
+//
+// All routines here are executed cooperatively by one thread block of
+// TTB_THREADS threads.  Matrices are addressed through generic pointers and
+// explicit (row, column) element strides, so the same code runs on shared
+// memory, on global memory and on transposed views.  Reductions are done in a
+// fixed order (per-thread strided partials, a warp tree, then the warp sums
+// in warp order), so a result never depends on scheduling and every thread
+// of the block sees the same value.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#ifndef TTB_THREADS
+#define TTB_THREADS 256
+#endif
+#define TTB_WARPS (TTB_THREADS / 32)
+
+namespace ttb {
+
+typedef long long i64;
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v) {
+  // tree towards lane 0, then broadcast lane 0 so all lanes agree bitwise
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Sum over the block; every thread returns the same value.  ``red`` must
+// hold TTB_WARPS doubles of shared memory.  Contains two __syncthreads.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int i = 0; i < TTB_WARPS; ++i) t += red[i];
+  return t;
+}
+
+// Index of the entry of largest absolute value, first index on ties (the
+// LAPACK idamax convention).  ``redv``/``redi`` hold TTB_WARPS entries.
+__device__ __forceinline__ int block_argmax_abs(double v, int idx, double* redv, int* redi) {
+  double a = (idx >= 0) ? fabs(v) : -1.0;
+  int i = idx;
+  for (int o = 16; o > 0; o >>= 1) {
+    double a2 = __shfl_down_sync(0xffffffffu, a, o);
+    int i2 = __shfl_down_sync(0xffffffffu, i, o);
+    if (a2 > a || (a2 == a && i2 >= 0 && (i < 0 || i2 < i))) { a = a2; i = i2; }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) { redv[wid] = a; redi[wid] = i; }
+  __syncthreads();
+  double best = -1.0;
+  int bi = -1;
+  for (int w = 0; w < TTB_WARPS; ++w) {
+    double a2 = redv[w];
+    int i2 = redi[w];
+    if (a2 > best || (a2 == best && i2 >= 0 && (bi < 0 || i2 < bi))) { best = a2; bi = i2; }
+  }
+  return bi;
+}
+
+// ---------------------------------------------------------------------------
+// strided matrix view
+// ---------------------------------------------------------------------------
+
+struct Mat {
+  double* p;
+  i64 rs, cs;  // element strides of a row step and a column step
+  __device__ __forceinline__ double& operator()(int i, int j) const { return p[i * rs + j * cs]; }
+};
+
+struct CMat {
+  const double* p;
+  i64 rs, cs;
+  __device__ __forceinline__ double operator()(int i, int j) const { return p[i * rs + j * cs]; }
+};
+
+// ---------------------------------------------------------------------------
+// GEMM: one 64x64 output tile per call, K staged through shared memory
+// ---------------------------------------------------------------------------
+
+constexpr int GBM = 64, GBN = 64, GBK = 16;
+
+struct GemmSmem {
+  double a[GBK][GBM + 1];
+  double b[GBK][GBN + 1];
+};
+
+// C[m0:m0+64, n0:n0+64] = alpha * A * B + beta * C over the full K range.
+// A is M x K, B is K x N.  beta == 0 never reads C.  Thread (tx, ty) of a
+// 16 x 16 grid owns rows ty + 16 i and columns tx + 16 j.
+__device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0, int n0,
+                              double alpha, double beta, GemmSmem& sm) {
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+  // loads walk the unit-stride direction of each operand when there is one
+  const bool a_kfast = (A.cs == 1);
+  const bool b_nfast = (B.cs == 1) || (B.rs != 1);
+  double ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int idx = tid + e * TTB_THREADS;
+      int mm, kk;
+      if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
+      int gm = m0 + mm, gk = k0 + kk;
+      ra[e] = (gm < M && gk < K) ? A(gm, gk) : 0.0;
+      int nn, kb;
+      if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
+      int gn = n0 + nn, gk2 = k0 + kb;
+      rb[e] = (gn < N && gk2 < K) ? B(gk2, gn) : 0.0;
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int idx = tid + e * TTB_THREADS;
+      int mm, kk;
+      if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
+      sm.a[kk][mm] = ra[e];
+      int nn, kb;
+      if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
+      sm.b[kb][nn] = rb[e];
+    }
+  };
+
+  if (K > 0) load(0);
+  for (int k0 = 0; k0 < K; k0 += GBK) {
+    __syncthreads();  // previous compute finished with the tile
+    store();
+    __syncthreads();
+    if (k0 + GBK < K) load(k0 + GBK);  // prefetch overlaps the FMAs below
+#pragma unroll
+    for (int k = 0; k < GBK; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = sm.a[k][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = sm.b[k][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx + 16 * j;
+      if (gn >= N) continue;
+      double v = alpha * acc[i][j];
+      if (beta != 0.0) v = fma(beta, C(gm, gn), v);
+      C(gm, gn) = v;
+    }
+  }
+  __syncthreads();  // callers may reuse the staging buffers right away
+}
+
+// Whole product, looping over all output tiles with the one block.
+__device__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
+                         GemmSmem& sm) {
+  for (int m0 = 0; m0 < M; m0 += GBM)
+    for (int n0 = 0; n0 < N; n0 += GBN) cta_gemm_tile(A, B, C, M, N, K, m0, n0, alpha, beta, sm);
+}
+
+// ---------------------------------------------------------------------------
+// copies
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cta_copy(CMat src, Mat dst, int M, int N, double alpha = 1.0) {
+  const int total = M * N;
+  // walk the unit-stride direction of the destination when there is one
+  const bool rowfast = (dst.cs == 1);
+  for (int e = threadIdx.x; e < total; e += TTB_THREADS) {
+    int i, j;
+    if (rowfast) { i = e / N; j = e % N; } else { i = e % M; j = e / M; }
+    dst(i, j) = alpha * src(i, j);
+  }
+}
+
+__device__ __forceinline__ void cta_fill(Mat dst, int M, int N, double v) {
+  const int total = M * N;
+  for (int e = threadIdx.x; e < total; e += TTB_THREADS) {
+    int i = e % M, j = e / M;
+    dst(i, j) = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR
+// ---------------------------------------------------------------------------
+
+// In-place Householder QR of the m x k matrix W (column step ``ldw``, unit
+// row step), as LAPACK dgeqr2 lays it out: on return R is in the upper
+// triangle and the reflector vectors v_j (v_j[j] = 1 implied) below the
+// diagonal, with the scalars in tau[0 .. min(m,k)-1].  Each reflector is
+// H = I - tau v v^T built as in dlarfg: beta = -sign(alpha) ||x||,
+// tau = (beta - alpha) / beta, v = x / (alpha - beta); a column whose
+// sub-diagonal part is exactly zero gets tau = 0.
+__device__ void cta_householder(double* W, int m, int k, i64 ldw, double* tau, double* red) {
+  const int p = m < k ? m : k;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int j = 0; j < p; ++j) {
+    double* col = W + j * ldw;
+    double part = 0.0;
+    for (int i = j + 1 + threadIdx.x; i < m; i += TTB_THREADS) part = fma(col[i], col[i], part);
+    double sigma = block_sum(part, red);
+    double alpha = col[j];
+    double t = 0.0, beta = alpha, scale = 0.0;
+    if (sigma != 0.0) {
+      double nrm = sqrt(alpha * alpha + sigma);
+      beta = (alpha >= 0.0) ? -nrm : nrm;
+      t = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    __syncthreads();  // everyone has read col[j] before it is overwritten
+    if (sigma != 0.0) {
+      for (int i = j + 1 + threadIdx.x; i < m; i += TTB_THREADS) col[i] *= scale;
+    }
+    if (threadIdx.x == 0) {
+      col[j] = beta;
+      tau[j] = t;
+    }
+    __syncthreads();
+    if (t != 0.0) {
+      // trailing update, one warp per column
+      for (int c = j + 1 + wid; c < k; c += TTB_WARPS) {
+        double* cc = W + c * ldw;
+        double w = 0.0;
+        for (int i = j + 1 + lane; i < m; i += 32) w = fma(col[i], cc[i], w);
+        w = warp_sum(w) + cc[j];
+        w *= t;
+        if (lane == 0) cc[j] -= w;
+        for (int i = j + 1 + lane; i < m; i += 32) cc[i] = fma(-w, col[i], cc[i]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Overwrite the m x q matrix X (strided) with H_0 H_1 ... H_{p-1} X, the
+// reflectors of cta_householder (applied last to first).
+__device__ void cta_apply_q(const double* W, int m, int p, i64 ldw, const double* tau, Mat X,
+                            int q) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int j = p - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t != 0.0) {
+      const double* v = W + j * ldw;
+      for (int c = wid; c < q; c += TTB_WARPS) {
+        double w = 0.0;
+        for (int i = j + 1 + lane; i < m; i += 32) w = fma(v[i], X(i, c), w);
+        w = warp_sum(w) + X(j, c);
+        w *= t;
+        if (lane == 0) X(j, c) -= w;
+        for (int i = j + 1 + lane; i < m; i += 32) X(i, c) = fma(-w, v[i], X(i, c));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Economic QR of the m x k matrix ``A`` (any strides): Q (m x p) and R
+// (p x k), p = min(m, k).  ``W`` is an m x k column-major work area (unit
+// row step, column step m), ``tau`` p doubles; both may be shared or
+// global memory.  Q and R may be NULL to skip them.
+__device__ void cta_qr(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R, double* red) {
+  const int p = m < k ? m : k;
+  cta_copy(A, Mat{W, 1, (i64)m}, m, k);
+  __syncthreads();
+  cta_householder(W, m, k, m, tau, red);
+  if (R.p) {
+    for (int e = threadIdx.x; e < p * k; e += TTB_THREADS) {
+      int i = e % p, j = e / p;
+      R(i, j) = (i <= j) ? W[i + (i64)j * m] : 0.0;
+    }
+  }
+  if (Q.p) {
+    for (int e = threadIdx.x; e < m * p; e += TTB_THREADS) {
+      int i = e % m, j = e / m;
+      Q(i, j) = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q(W, m, p, m, tau, Q, p);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// one-sided Jacobi SVD of a small square matrix
+// ---------------------------------------------------------------------------
+
+// Hestenes one-sided Jacobi on the columns of the k x k matrix B (column
+// major, leading dimension ldb): finds an orthogonal V with B V having
+// orthogonal columns.  On return B holds B V and V (column major, ldv) the
+// accumulated rotations.  Pairs are visited in round-robin tournament order
+// (k/2 disjoint pairs per round, one warp per pair).  A pair is rotated when
+// |b_p . b_q| > tol sqrt(|b_p|^2 |b_q|^2); sweeps stop when one sweep
+// rotates nothing, or after ``max_sweeps``.  Returns the sweeps used, or -1
+// when the cap was hit.
+__device__ int cta_jacobi(double* B, int k, i64 ldb, double* V, i64 ldv, int max_sweeps,
+                          double tol, int* flag) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < k * k; e += TTB_THREADS) {
+    int i = e % k, j = e / k;
+    V[i + j * ldv] = (i == j) ? 1.0 : 0.0;
+  }
+  if (k < 2) {
+    __syncthreads();
+    return 0;
+  }
+  const int kk = (k + 1) & ~1;  // players, one dummy when k is odd
+  const int half = kk / 2;
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    if (threadIdx.x == 0) *flag = 0;
+    __syncthreads();
+    int rotated = 0;
+    for (int round = 0; round < kk - 1; ++round) {
+      for (int pr = wid; pr < half; pr += TTB_WARPS) {
+        int pa = (pr == 0) ? 0 : ((pr - 1 + round) % (kk - 1)) + 1;
+        int pos = kk - 1 - pr;
+        int pb = ((pos - 1 + round) % (kk - 1)) + 1;
+        int p = pa < pb ? pa : pb, q = pa < pb ? pb : pa;
+        if (q >= k) continue;  // paired with the dummy player
+        double* bp = B + p * ldb;
+        double* bq = B + q * ldb;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = lane; i < k; i += 32) {
+          double x = bp[i], y = bq[i];
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        ga = warp_sum(ga);
+        if (ga != 0.0 && fabs(ga) > tol * sqrt(al) * sqrt(be)) {
+          double zeta = (be - al) / (2.0 * ga);
+          double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          double c = 1.0 / sqrt(1.0 + t * t);
+          double s = c * t;
+          for (int i = lane; i < k; i += 32) {
+            double x = bp[i], y = bq[i];
+            bp[i] = c * x - s * y;
+            bq[i] = s * x + c * y;
+          }
+          double* vp = V + p * ldv;
+          double* vq = V + q * ldv;
+          for (int i = lane; i < k; i += 32) {
+            double x = vp[i], y = vq[i];
+            vp[i] = c * x - s * y;
+            vq[i] = s * x + c * y;
+          }
+          rotated = 1;
+        }
+      }
+      __syncthreads();
+    }
+    if (rotated) *flag = 1;  // benign race: every writer stores 1
+    __syncthreads();
+    int any = *flag;
+    __syncthreads();
+    if (!any) return sweep + 1;
+  }
+  return -1;
+}
+
+// Thin SVD of the m x k matrix A (any strides), m >= k required, as
+// A = U diag(S) Vh with S descending: Householder QR A = Q R, one-sided
+// Jacobi on R (R V = B, columns of B orthogonal), singular values the
+// column norms of B, U = Q [B diag(1/S); 0].  Work areas (shared or global):
+// W (m x k, column major), tau (k), Bsq (k x k), V (k x k), sv (k),
+// order (k ints), flag (1 int).  U (m x k), S (k) and Vh (k x k) are
+// strided outputs; U is also used as the work area of the final Q product.
+// Returns the Jacobi sweeps used, or -1 if the sweep cap was hit.
+__device__ int cta_svd_tall(CMat A, int m, int k, double* W, double* tau, double* Bsq, double* V,
+                            double* sv, int* order, int* flag, Mat U, double* S, Mat Vh,
+                            double* red) {
+  cta_copy(A, Mat{W, 1, (i64)m}, m, k);
+  __syncthreads();
+  cta_householder(W, m, k, m, tau, red);
+  for (int e = threadIdx.x; e < k * k; e += TTB_THREADS) {
+    int i = e % k, j = e / k;
+    Bsq[i + (i64)j * k] = (i <= j) ? W[i + (i64)j * m] : 0.0;
+  }
+  __syncthreads();
+  const double tol = 4.0 * k * 2.220446049250313e-16;
+  int status = cta_jacobi(Bsq, k, k, V, k, 60, tol, flag);
+  for (int j = threadIdx.x; j < k; j += TTB_THREADS) {
+    double s = 0.0;
+    for (int i = 0; i < k; ++i) s = fma(Bsq[i + (i64)j * k], Bsq[i + (i64)j * k], s);
+    sv[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += TTB_THREADS) {
+    double sj = sv[j];
+    int rank = 0;
+    for (int i = 0; i < k; ++i) {
+      double si = sv[i];
+      rank += (si > sj) || (si == sj && i < j);
+    }
+    order[rank] = j;
+  }
+  __syncthreads();
+  // U <- [B(:, order) / S ; 0], S and Vh in descending order
+  for (int e = threadIdx.x; e < m * k; e += TTB_THREADS) {
+    int i = e % m, r = e / m;
+    int j = order[r];
+    double sj = sv[j];
+    double v;
+    if (i < k) v = (sj > 0.0) ? Bsq[i + (i64)j * k] / sj : (i == r ? 1.0 : 0.0);
+    else v = 0.0;
+    U(i, r) = v;
+  }
+  for (int r = threadIdx.x; r < k; r += TTB_THREADS) S[r] = sv[order[r]];
+  for (int e = threadIdx.x; e < k * k; e += TTB_THREADS) {
+    int r = e % k, c = e / k;
+    Vh(r, c) = V[c + (i64)order[r] * k];
+  }
+  __syncthreads();
+  cta_apply_q(W, m, k, m, tau, U, k);
+  return status;
+}
+
+// Gaussian elimination with partial pivoting on [W | b] (LAPACK getrf/getrs
+// semantics: largest |pivot|, first index on ties), W column major with
+// leading dimension ld, then back substitution.  b is overwritten with the
+// solution and W with the factors.  Returns 0, or the 1-based index of the
+// first exactly-zero pivot (the solve then stops, like gesv's info > 0).
+__device__ int cta_gepp_solve(double* W, i64 ld, double* b, int n, double* redv, int* redi) {
+  for (int j = 0; j < n; ++j) {
+    double best = -1.0;
+    int bi = -1;
+    for (int i = j + threadIdx.x; i < n; i += TTB_THREADS) {
+      double a = fabs(W[i + j * ld]);
+      if (a > best) { best = a; bi = i; }
+    }
+    int piv = block_argmax_abs(best, bi, redv, redi);
+    if (piv != j) {
+      for (int c = j + threadIdx.x; c < n; c += TTB_THREADS) {
+        double t = W[j + c * ld];
+        W[j + c * ld] = W[piv + c * ld];
+        W[piv + c * ld] = t;
+      }
+      if (threadIdx.x == 0) {
+        double t = b[j];
+        b[j] = b[piv];
+        b[piv] = t;
+      }
+    }
+    __syncthreads();
+    const double d = W[j + j * ld];
+    if (d == 0.0) return j + 1;
+    const double rd = 1.0 / d;
+    for (int i = j + 1 + threadIdx.x; i < n; i += TTB_THREADS) W[i + j * ld] *= rd;
+    __syncthreads();
+    const int rows = n - j - 1;
+    const int total = rows * rows;
+    for (int e = threadIdx.x; e < total; e += TTB_THREADS) {
+      int i = j + 1 + e % rows, c = j + 1 + e / rows;
+      W[i + c * ld] = fma(-W[i + j * ld], W[j + c * ld], W[i + c * ld]);
+    }
+    const double bj = b[j];
+    for (int i = j + 1 + threadIdx.x; i < n; i += TTB_THREADS) b[i] = fma(-W[i + j * ld], bj, b[i]);
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (threadIdx.x == 0) b[j] = b[j] / W[j + j * ld];
+    __syncthreads();
+    const double xj = b[j];
+    for (int i = threadIdx.x; i < j; i += TTB_THREADS) b[i] = fma(-W[i + j * ld], xj, b[i]);
+    __syncthreads();
+  }
+  return 0;
+}
+
+}  // namespace ttb

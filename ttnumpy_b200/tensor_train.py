@@ -1,0 +1,515 @@
+"""Device-resident tensor train with the reference container's interface.
+
+``TensorTrain`` keeps its cores as CUDA float64 tensors of shape
+``(r_k, row_mode_k, col_mode_k, r_{k+1})`` (the reference layout,
+``ttnumpy/tensor_train.py:150-244``).  Rounding (``truncate``,
+``orthonormalize``, ``compress_svd``), the TTM-by-TT product (``dot``), sums
+and norms run on the GPU through libttb200; only rank decisions and norms
+come back to the host.  Constructors take host NumPy arrays (input
+preparation is host work in the reference too) and upload them.
+"""
+
+from __future__ import annotations
+
+import logging
+import math
+import numbers
+from enum import Enum
+from typing import List, Optional, Tuple, Union
+
+import numpy as np
+import torch
+
+from . import kernels as K
+
+logger = logging.getLogger("ttnumpy")
+
+
+class DimensionMismatch(Exception):
+    """Exception for dimension errors (``tensor_train.py:21-26``)."""
+
+    def __init__(self, msg="Dimension mismatch"):
+        self.msg = msg
+        super().__init__(self.msg)
+
+
+class WrongTTFormat(Exception):
+    """Exception for an invalid train structure (``tensor_train.py:29-34``)."""
+
+    def __init__(self, msg="Wrong tensor train format"):
+        self.msg = msg
+        super().__init__(self.msg)
+
+
+class WrongTTType(Exception):
+    """Exception for a TT where a TTM is needed or vice versa
+    (``tensor_train.py:37-42``)."""
+
+    def __init__(self, msg="Wrong tensor train type"):
+        self.msg = msg
+        super().__init__(self.msg)
+
+
+class TensorTrainType(Enum):
+    TT = "Tensor Train"
+    TTM = "Tensor Train Matrix"
+
+
+def _to_device(core) -> torch.Tensor:
+    if isinstance(core, torch.Tensor):
+        t = core.to(device="cuda", dtype=torch.float64)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(core, dtype=np.float64))).to("cuda")
+    return t.contiguous()
+
+
+def _mat(core: torch.Tensor, rows: int) -> torch.Tensor:
+    return core.reshape(rows, -1)
+
+
+class TensorTrain:
+    """Tensor train (TT) or tensor train matrix (TTM) on the GPU.
+
+    Validation and attributes follow the reference constructor
+    (``tensor_train.py:169-244``).
+    """
+
+    __array_ufunc__ = None
+
+    def __init__(self, cores: List, orth_center: Optional[int] = None):
+        K.device_ok()
+        if len(cores) < 2:
+            raise WrongTTFormat("Tensor train must has at least 2 sites")
+        ndims = {len(c.shape) for c in cores}
+        if ndims == {3}:
+            cores = [_to_device(c).reshape(c.shape[0], c.shape[1], 1, c.shape[2]) for c in cores]
+        elif ndims == {4}:
+            cores = [_to_device(c) for c in cores]
+        else:
+            raise WrongTTFormat("All cores must be 3 or 4 rank tensors")
+        tt_type = (TensorTrainType.TT if all(c.shape[2] == 1 for c in cores)
+                   else TensorTrainType.TTM)
+        bonds = [1]
+        for i, core in enumerate(cores):
+            if i == 0 and core.shape[0] != 1:
+                raise WrongTTFormat("Only open boundary conditions is supported, first core "
+                                    "must has first index equal to 1")
+            if i == len(cores) - 1 and core.shape[-1] != 1:
+                raise WrongTTFormat("Only open boundary conditions is supported, last core "
+                                    "must has last index equal to 1")
+            if core.shape[0] != bonds[i]:
+                raise DimensionMismatch(
+                    f"Connected sites bonds are mismatching: {core.shape[0]} != {bonds[i]}")
+            bonds.append(core.shape[-1])
+        self.cores = cores
+        self.tt_type = tt_type
+        self.orth_center = orth_center
+
+    # -- attributes ---------------------------------------------------------
+
+    @property
+    def n_cores(self) -> int:
+        return len(self.cores)
+
+    @property
+    def bonds(self) -> List[int]:
+        return [int(c.shape[0]) for c in self.cores] + [1]
+
+    @property
+    def row_modes(self) -> List[int]:
+        return [int(c.shape[1]) for c in self.cores]
+
+    @property
+    def col_modes(self) -> List[int]:
+        if self.tt_type is TensorTrainType.TT:
+            return [1] * len(self.cores)
+        return [int(c.shape[2]) for c in self.cores]
+
+    @property
+    def max_rank(self) -> int:
+        return max(self.bonds)
+
+    def __len__(self) -> int:
+        return len(self.cores)
+
+    def __getitem__(self, idx):
+        return self.cores[idx]
+
+    def is_ttm(self) -> bool:
+        return self.tt_type is TensorTrainType.TTM
+
+    def physical_dims(self) -> List:
+        if self.tt_type is TensorTrainType.TT:
+            return self.row_modes
+        return list(zip(self.row_modes, self.col_modes))
+
+    def copy(self) -> "TensorTrain":
+        out = TensorTrain.__new__(TensorTrain)
+        out.cores = [c.clone() for c in self.cores]
+        out.tt_type = self.tt_type
+        out.orth_center = self.orth_center
+        return out
+
+    @classmethod
+    def _wrap(cls, cores: List[torch.Tensor], orth_center=None) -> "TensorTrain":
+        out = cls.__new__(cls)
+        out.cores = cores
+        out.tt_type = (TensorTrainType.TT if all(c.shape[2] == 1 for c in cores)
+                       else TensorTrainType.TTM)
+        out.orth_center = orth_center
+        return out
+
+    # -- host transfer ------------------------------------------------------
+
+    def to_numpy(self) -> List[np.ndarray]:
+        return [c.detach().cpu().numpy() for c in self.cores]
+
+    def get_full_tensor(self) -> np.ndarray:
+        """Dense tensor on the host (a convenience for small trains; the
+        contraction order of ``tensor_train.py:599-624``)."""
+        cores = self.to_numpy()
+        t = cores[0].reshape(-1, cores[0].shape[-1])
+        for c in cores[1:]:
+            t = (t @ c.reshape(c.shape[0], -1)).reshape(-1, c.shape[-1])
+        t = t.reshape(-1)
+        if self.is_ttm():
+            shape = [x for p in zip(self.row_modes, self.col_modes) for x in p]
+            t = t.reshape(shape)
+            d = len(self.cores)
+            perm = list(range(0, 2 * d, 2)) + list(range(1, 2 * d, 2))
+            return t.transpose(perm)
+        shape = self.row_modes
+        if shape == [1] * len(shape):
+            return t.item()
+        return t.reshape(shape)
+
+    # -- arithmetic ---------------------------------------------------------
+
+    def add(self, other: "TensorTrain", truncate: bool = False, error=None, max_rank=None,
+            method: str = "direct", seed=None, options=None) -> "TensorTrain":
+        """Block-diagonal sum (``tensor_train.py:254-322``)."""
+        if not isinstance(other, TensorTrain):
+            raise TypeError(
+                f"unsupported operand type(s) for +: 'TensorTrain' and '{type(other)}'")
+        if self.physical_dims() != other.physical_dims():
+            raise DimensionMismatch("Tensor trains must have the same dimensions")
+        d = len(self)
+        ra, rb = self.bonds, other.bonds
+        ranks = [1] + [ra[i] + rb[i] for i in range(1, d)] + [1]
+        cores, descs = [], []
+        for i in range(d):
+            a, b = self.cores[i], other.cores[i]
+            out = torch.empty(ranks[i], a.shape[1], a.shape[2], ranks[i + 1], dtype=torch.float64,
+                              device="cuda")
+            descs.append(K.copy_desc(None, out, 0.0))
+            cores.append(out)
+        K.copy_many(descs)
+        descs = []
+        for i in range(d):
+            a, b, out = self.cores[i], other.cores[i], cores[i]
+            descs.append(K.copy_desc(a, out[: ra[i], :, :, : ra[i + 1]]))
+            descs.append(K.copy_desc(b, out[ranks[i] - rb[i]:, :, :, ranks[i + 1] - rb[i + 1]:]))
+        K.copy_many(descs)
+        res = TensorTrain._wrap(cores)
+        return _round_result(res, truncate, error, max_rank, method)
+
+    def __add__(self, other):
+        return self.add(other)
+
+    def multiply(self, other, truncate: bool = False, error=None, max_rank=None,
+                 method: str = "direct", seed=None, options=None) -> "TensorTrain":
+        """Scalar multiple (``tensor_train.py:389-395``); the element-wise
+        product of two trains is not part of the solve path."""
+        if isinstance(other, numbers.Number) and not isinstance(other, bool):
+            res = self.copy()
+            k = res.orth_center if res.orth_center is not None else 0
+            K.copy_(res.cores[k], self.cores[k], float(other))
+            return _round_result(res, truncate, error, max_rank, method)
+        if isinstance(other, TensorTrain):
+            raise NotImplementedError("element-wise products of two trains are not on the "
+                                      "tensor-train solve path")
+        raise TypeError(f"unsupported operand type(s) for *: 'TensorTrain' and '{type(other)}'")
+
+    def __mul__(self, other):
+        return self.multiply(other)
+
+    def __rmul__(self, other):
+        return self.multiply(other)
+
+    def __neg__(self):
+        return self.multiply(-1)
+
+    def __sub__(self, other):
+        return self.add(-other)
+
+    def dot(self, other: "TensorTrain", truncate: bool = False, error=None, max_rank=None,
+            method: str = "direct", seed=None, options=None) -> "TensorTrain":
+        """TTM-by-TT (or TTM-by-TTM) product, Kronecker cores built on the
+        device (``tensor_train.py:427-499``)."""
+        if not isinstance(other, TensorTrain):
+            raise TypeError(
+                f"unsupported operand type(s) for @: 'TensorTrain' and '{type(other)}'")
+        if self.col_modes != other.row_modes:
+            raise DimensionMismatch("Tensor trains must have the same last and first physical "
+                                    "dimensions respectively")
+        cores = [K.kron(a, x) for a, x in zip(self.cores, other.cores)]
+        return _round_result(TensorTrain._wrap(cores), truncate, error, max_rank, method)
+
+    def __matmul__(self, other):
+        return self.dot(other)
+
+    # -- norms and canonical forms ------------------------------------------
+
+    def tt_norm(self) -> float:
+        """Frobenius norm; the centre core's norm when ``orth_center`` is
+        set, else a right QR sweep that keeps only the R factors
+        (``tensor_train.py:509-540``)."""
+        out = K.empty(1)
+        if self.orth_center is not None:
+            K.norm_into(out, self.cores[self.orth_center])
+            return float(out.item())
+        carry = None
+        for i in range(len(self) - 1, 0, -1):
+            c = self.cores[i]
+            m = c if carry is None else _apply_right(c, carry)
+            mat = _mat(m, m.shape[0])
+            _, r = K.qr(mat.t(), want_q=False)
+            carry = r.t()  # (r_i, p) : previous core @ carry
+        first = _apply_right(self.cores[0], carry)
+        K.norm_into(out, first)
+        return float(out.item())
+
+    def orthonormalize(self, canonical: str = "left", center_position: Optional[int] = None,
+                       inplace: bool = False) -> "TensorTrain":
+        """QR canonicalisation (``tensor_train.py:705-787``)."""
+        d = len(self)
+        if center_position is not None and not 0 <= center_position < d:
+            raise ValueError(f"center_position must be in [0, {d - 1}], but got {center_position}")
+        t = self if inplace else self.copy()
+        had_center = t.orth_center is not None
+        if canonical == "left":
+            end = center_position if center_position is not None else d - 1
+            start = 0
+            if t.orth_center is not None:
+                start = t.orth_center
+                if start <= end:
+                    t.orth_center = end
+            if start >= end:
+                return t
+            left_orth_sweep(t.cores, start, end)
+        elif canonical == "right":
+            end = center_position if center_position is not None else 0
+            start = d - 1
+            if t.orth_center is not None:
+                start = t.orth_center
+                if start >= end:
+                    t.orth_center = end
+            if start <= end:
+                return t
+            right_orth_sweep(t.cores, start, end)
+        elif canonical == "mix":
+            if center_position is None:
+                center_position = d // 2
+            end = center_position
+            left_orth_sweep(t.cores, 0, center_position)
+            right_orth_sweep(t.cores, d - 1, center_position)
+        else:
+            raise ValueError(
+                f"Canonical form must be 'left', 'right' or 'mix', but got {canonical}")
+        if had_center or canonical == "mix" or end in (0, d - 1):
+            t.orth_center = end
+        else:
+            t.orth_center = None
+        return t
+
+    def compress_svd(self, error: float = 0.0, max_rank: Optional[int] = None,
+                     canonical: str = "auto", inplace: bool = False) -> "TensorTrain":
+        """SVD truncation sweep (``tensor_train.py:789-850``)."""
+        t = self if inplace else self.copy()
+        d = len(t)
+        if canonical == "auto":
+            canonical = ("left" if (t.orth_center is None or t.orth_center <= (d - 1) / 2)
+                         else "right")
+        if canonical == "right":
+            right_svd_sweep(t.cores, error, max_rank)
+            t.orth_center = 0
+        elif canonical == "left":
+            left_svd_sweep(t.cores, error, max_rank)
+            t.orth_center = d - 1
+        else:
+            raise ValueError(
+                f"Canonical form must be 'left', 'right' or 'auto', but got {canonical}")
+        return t
+
+    def truncate(self, error: float = 0.0, max_rank: Optional[int] = None,
+                 canonical: str = "auto", inplace: bool = False, method: str = "direct",
+                 seed=None, options=None) -> "TensorTrain":
+        """Round to minimal ranks: QR canonicalisation then the SVD sweep
+        (``tensor_train.py:852-940``, ``method="direct"``)."""
+        if canonical not in ("auto", "left", "right"):
+            raise ValueError(
+                f"Canonical form must be 'left', 'right' or 'auto', but got {canonical}")
+        if method not in ("direct", "randomized"):
+            raise ValueError(f"Method must be 'direct' or 'randomized', but got {method!r}")
+        if method == "randomized":
+            raise NotImplementedError("randomized rounding is not part of the solve path")
+        t = self if inplace else self.copy()
+        orth_form = "left" if canonical == "right" else "right"
+        if canonical == "auto":
+            if t.orth_center is None or t.orth_center >= len(t) / 2:
+                orth_form = "left"
+            else:
+                orth_form = "right"
+        t.orthonormalize(canonical=orth_form, inplace=True)
+        t.compress_svd(error, max_rank, inplace=True)
+        return t
+
+    def __str__(self):
+        return (f"{self.tt_type.value} with following properties:\n\t Number of cores: "
+                f"{len(self)}\n\t Bonds: {self.bonds}\n\t Physical indexes: "
+                f"{self.physical_dims()}")
+
+
+def _round_result(res, truncate, error, max_rank, method):
+    """``_round_result`` (``tensor_train.py:94-119``)."""
+    if not truncate:
+        if method != "direct" or error is not None or max_rank is not None:
+            raise ValueError("error, max_rank and method need truncate=True")
+        return res
+    return res.truncate(error=0.0 if error is None else error, max_rank=max_rank, inplace=True,
+                        method=method)
+
+
+# ---------------------------------------------------------------------------
+# sweeps on lists of device cores (utils.py:86-136, 364-460)
+# ---------------------------------------------------------------------------
+
+
+def _apply_left(matrix: torch.Tensor, core: torch.Tensor) -> torch.Tensor:
+    """``matrix @ core`` over the first core axis (``utils.py:72-76``)."""
+    out = torch.empty((matrix.shape[0],) + tuple(core.shape[1:]), dtype=torch.float64,
+                      device="cuda")
+    K.gemm(matrix, core.reshape(core.shape[0], -1), out.view(matrix.shape[0], -1))
+    return out
+
+
+def _apply_right(core: torch.Tensor, matrix: torch.Tensor) -> torch.Tensor:
+    """``core @ matrix`` over the last core axis (``utils.py:79-83``)."""
+    out = torch.empty(tuple(core.shape[:-1]) + (matrix.shape[1],), dtype=torch.float64,
+                      device="cuda")
+    K.gemm(core.reshape(-1, core.shape[-1]), matrix, out.view(-1, matrix.shape[1]))
+    return out
+
+
+def left_orth_sweep(cores: List[torch.Tensor], start: int, end: int) -> None:
+    for i in range(start, end):
+        s = cores[i].shape
+        q, r = K.qr(cores[i].reshape(s[0] * s[1] * s[2], s[3]))
+        cores[i] = q.reshape(s[0], s[1], s[2], q.shape[1])
+        cores[i + 1] = _apply_left(r, cores[i + 1])
+
+
+def right_orth_sweep(cores: List[torch.Tensor], start: int, end: int) -> None:
+    for i in range(start, end, -1):
+        s = cores[i].shape
+        rest = s[1] * s[2] * s[3]
+        p = min(rest, s[0])
+        qt = K.empty(p, rest)  # Q^T, written through a transposed view
+        _, r = K.qr(cores[i].reshape(s[0], rest).t(), q_out=qt.t())
+        cores[i] = qt.reshape(p, s[1], s[2], s[3])
+        cores[i - 1] = _apply_right(cores[i - 1], r.t())
+
+
+def _svd_rank(s: torch.Tensor, delta: float, max_rank) -> int:
+    rk = torch.empty(1, dtype=torch.int32, device="cuda")
+    K.rank_threshold(s, 1, delta, max_rank, rk)
+    return int(rk.item())
+
+
+def left_svd_sweep(cores: List[torch.Tensor], error: float, max_rank=None) -> None:
+    if max_rank is not None and max_rank <= 0:
+        raise ValueError("max_rank must be a positive integer.")
+    nrm = K.empty(1)
+    K.norm_into(nrm, cores[0])
+    delta = error / math.sqrt(len(cores) - 1) * float(nrm.item())
+    for i in range(len(cores) - 1):
+        s = cores[i].shape
+        u, sv, vh = K.svd(cores[i].reshape(s[0] * s[1] * s[2], s[3]))
+        nb = _svd_rank(sv, delta, max_rank)
+        core = K.empty(s[0], s[1], s[2], nb)
+        K.copy_(core.view(-1, nb), u[:, :nb])
+        carry = K.empty(nb, s[3])
+        K.copy_(carry, vh[:nb], scale=sv, scale_axis=0)
+        cores[i] = core
+        cores[i + 1] = _apply_left(carry, cores[i + 1])
+
+
+def right_svd_sweep(cores: List[torch.Tensor], error: float, max_rank=None) -> None:
+    if max_rank is not None and max_rank <= 0:
+        raise ValueError("max_rank must be a positive integer.")
+    nrm = K.empty(1)
+    K.norm_into(nrm, cores[-1])
+    delta = error / math.sqrt(len(cores) - 1) * float(nrm.item())
+    for i in range(len(cores) - 1, 0, -1):
+        s = cores[i].shape
+        u, sv, vh = K.svd(cores[i].reshape(s[0], s[1] * s[2] * s[3]))
+        nb = _svd_rank(sv, delta, max_rank)
+        core = K.empty(nb, s[1], s[2], s[3])
+        K.copy_(core.view(nb, -1), vh[:nb])
+        carry = K.empty(s[0], nb)
+        K.copy_(carry, u[:, :nb], scale=sv, scale_axis=1)
+        cores[i] = core
+        cores[i - 1] = _apply_right(cores[i - 1], carry)
+
+
+# ---------------------------------------------------------------------------
+# constructors (tensor_train.py:1250-1387), host-generated and uploaded
+# ---------------------------------------------------------------------------
+
+
+def _ranks(n: int, ranks) -> List[int]:
+    if isinstance(ranks, list):
+        return ranks
+    return [1] + [int(ranks)] * (n - 1) + [1]
+
+
+def _mode_pairs(physical_indexes):
+    if isinstance(physical_indexes[0], (int, np.integer)):
+        return [(int(p), 1) for p in physical_indexes]
+    return [(int(a), int(b)) for a, b in physical_indexes]
+
+
+def ones(physical_indexes, ranks=1) -> TensorTrain:
+    if len(physical_indexes) < 2:
+        raise WrongTTFormat("Tensor train must have at least two cores.")
+    r = _ranks(len(physical_indexes), ranks)
+    modes = _mode_pairs(physical_indexes)
+    return TensorTrain([np.ones((r[i], modes[i][0], modes[i][1], r[i + 1]))
+                        for i in range(len(modes))])
+
+
+def zeros(physical_indexes, ranks=1) -> TensorTrain:
+    if len(physical_indexes) < 2:
+        raise WrongTTFormat("Tensor train must have at least two cores.")
+    r = _ranks(len(physical_indexes), ranks)
+    modes = _mode_pairs(physical_indexes)
+    return TensorTrain([np.zeros((r[i], modes[i][0], modes[i][1], r[i + 1]))
+                        for i in range(len(modes))])
+
+
+def eye(physical_indexes) -> TensorTrain:
+    if len(physical_indexes) < 2:
+        raise WrongTTFormat("Tensor train must have at least two cores.")
+    return TensorTrain([np.eye(p).reshape(1, p, p, 1) for p in physical_indexes])
+
+
+def rand(physical_indexes, ranks=1, seed=None) -> TensorTrain:
+    """Uniform [0, 1) cores from ``np.random.default_rng(seed)``, drawn core
+    by core exactly as the reference does, then uploaded."""
+    if len(physical_indexes) < 2:
+        raise WrongTTFormat("Tensor train must have at least two cores.")
+    rng = np.random.default_rng(seed)
+    r = _ranks(len(physical_indexes), ranks)
+    modes = _mode_pairs(physical_indexes)
+    return TensorTrain([rng.random((r[i], modes[i][0], modes[i][1], r[i + 1]))
+                        for i in range(len(modes))])
