@@ -1,0 +1,522 @@
+#!/usr/bin/env python
+"""AMEn solves/s and p50/p99 latency at relative residual 1e-8 on B200.
+
+One step = solving one batch of synthetic requests (a seeded mix of 2-D QTT
+Poisson problems with 6-20 cores and parametric diffusion problems with
+d in {4, 5}, n in {16, 32}), each to relative residual 1e-8.  The requests
+are identical in every step.  ``--engine plain`` solves them one at a time
+through the drop-in ``amen``; ``--engine served`` (the default once
+available) admits all of them into the batched serving engine.
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
+(the NumPy/SciPy restatement of the reference path) on the host cores
+instead, on a bounded sample of the same requests.
+
+Launch: ``python bench.py`` (1 GPU) or, for N GPUs,
+``python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N``:
+every rank serves its own copy of the request batch (replicas; independent
+solves need no collective), ``value`` = all ranks' solves / max time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "AMEn solves/s at relative residual 1e-8"
+UNIT = "solves/s"
+TOL = 1e-8
+MAX_SWEEPS = 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "plain", "served"])
+    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="requests in the CPU baseline sample (0: automatic)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+
+def make_requests(count: int, seed: int):
+    """Seeded request mix: half 2-D QTT Poisson (N ~ U{3..10}, sin*sin
+    right-hand side), half parametric diffusion (d ~ U{4,5}, n ~ U{16,32},
+    theta ~ U(-1, 1))."""
+    from ttnumpy_b200 import problems as P
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        if i % 2 == 0:
+            N = int(rng.integers(3, 11))
+            p = P.qtt_poisson_2d(N)
+            p.meta["kind"] = "qtt"
+        else:
+            d = int(rng.integers(4, 6))
+            n = int(rng.choice((16, 32)))
+            p = P.parametric_diffusion(d, n, rng.uniform(-1.0, 1.0, size=d))
+            p.meta["kind"] = "diffusion"
+        reqs.append(p)
+    return reqs
+
+
+def solve_kwargs(p):
+    return dict(residual_tol=TOL, symmetric=True, max_sweeps=MAX_SWEEPS, seed=0,
+                stagnation_factor=None)
+
+
+def x0_cores(p):
+    """Initial guess: rank-3 all-ones for QTT Poisson (the reference
+    benchmark's choice), the default (all-ones with b's ranks) otherwise."""
+    if p.meta.get("kind") == "qtt":
+        return 3
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+
+
+def _cpu_solve(p):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    from threadpoolctl import threadpool_limits
+
+    from oracle import tt_oracle as O
+
+    with threadpool_limits(1):
+        A, b = O.Train(p.A), O.Train(p.b)
+        x0 = None
+        r = x0_cores(p)
+        if r is not None:
+            x0 = O.orthonormalize(O.ones(b.row_modes, ranks=r), "right")
+        t0 = time.perf_counter()
+        x, info = O.amen(A, b, x0=x0, **solve_kwargs(p))
+        dt = time.perf_counter() - t0
+    return dt, info.stop_reason, (info.residuals[-1] if info.residuals else float("nan"))
+
+
+def cpu_run(reqs, workers: int):
+    """Solve ``reqs`` on a spawn pool of single-threaded workers; returns
+    (seconds, per-request results)."""
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(workers) as pool:
+        res = pool.map(_cpu_solve, reqs, chunksize=1)
+    return time.perf_counter() - t0, res
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(reqs, n):
+    # every other request is QTT, so a prefix keeps the mix
+    return reqs[: max(2, n)]
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [v.strip() for v in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except OSError:
+        return {}
+
+
+def fp64_peak_tflops(K, torch):
+    """Measured FP64 FMA throughput of this GPU (own probe kernel)."""
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    lib = K.lib()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    lib.ttb_fma_peak(out.data_ptr(), blocks, iters, K.stream())
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        lib.ttb_fma_peak(out.data_ptr(), blocks, iters, K.stream())
+        b.record()
+        torch.cuda.synchronize()
+        flops = 2.0 * 8 * iters * 256 * blocks
+        best = max(best, flops / (a.elapsed_time(b) * 1e-3) / 1e12)
+    return best
+
+
+class Engine:
+    """Solves a list of requests; returns per-request latencies (ms)."""
+
+    def __init__(self, kind: str):
+        import torch
+
+        import ttnumpy_b200 as tt
+
+        self.kind = kind
+        self.tt = tt
+        self.torch = torch
+
+    def upload(self, reqs):
+        tt = self.tt
+        out = []
+        for p in reqs:
+            A, b = tt.TensorTrain(p.A), tt.TensorTrain(p.b)
+            r = x0_cores(p)
+            x0 = tt.ones(b.physical_dims(), ranks=r).orthonormalize("right") if r else None
+            out.append((A, b, x0, p))
+        return out
+
+    def solve_all(self, dev_reqs, download: bool = False):
+        torch = self.torch
+        lat = []
+        results = []
+        if self.kind == "plain":
+            for A, b, x0, p in dev_reqs:
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
+                x, info = self.tt.amen(A, b, x0=x0, return_info=True, **solve_kwargs(p))
+                if download:
+                    x.to_numpy()
+                e.record()
+                results.append((x, info))
+                lat.append((s, e))
+            torch.cuda.synchronize()
+            lat = [s.elapsed_time(e) for s, e in lat]
+        else:
+            from ttnumpy_b200.serving import serve_batch
+
+            results, lat = serve_batch(dev_reqs, solve_kwargs, download=download)
+        return results, lat
+
+
+def flush_l2(torch, buf):
+    from ttnumpy_b200 import kernels as K
+
+    K.fill_(buf, 0.0)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    reqs = make_requests(args.requests, args.seed)
+    cores = cpu_cores()
+    n_sample = args.cpu_sample or min(len(reqs), max(2 * cores, 8))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sample = cpu_sample(reqs, n_sample)
+        for _ in range(args.warmup):
+            cpu_run(sample[: min(len(sample), cores)], cores)
+        total, n = 0.0, 0
+        for _ in range(args.steps):
+            dt, res = cpu_run(sample, cores)
+            total += dt
+            n += sum(1 for r in res if str(r[1]) == "converged")
+        value = n / total
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config(args, reqs),
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                                 "sample": f"{len(sample)} of the {len(reqs)} requests per step "
+                                           f"(the first ones, same mix), {cores} single-threaded "
+                                           "oracle workers"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from ttnumpy_b200 import kernels as K
+
+    K.lib()
+    engine_kind = args.engine
+    if engine_kind == "auto":
+        try:
+            import ttnumpy_b200.serving  # noqa: F401
+
+            engine_kind = "served"
+        except ImportError:
+            engine_kind = "plain"
+    eng = Engine(engine_kind)
+    dev_reqs = eng.upload(reqs)
+    flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB > L2
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        eng.solve_all(dev_reqs)
+    barrier()
+
+    # which kernel class dominates: one profiled pass, all classes
+    lib = K.lib()
+    lib.ttb_profile_reset()
+    lib.ttb_profile_enable((1 << 12) - 1)
+    eng.solve_all(dev_reqs)
+    torch.cuda.synchronize()
+    lib.ttb_profile_enable(0)
+    shares = profile_read(lib)
+    dominant = max(shares, key=lambda c: shares[c]["ms"])
+    lib.ttb_profile_reset()
+
+    # timed region: device time per step, L2 flushed between steps
+    step_ms, lats, ok, launches = [], [], 0, 0
+    barrier()
+    with ClockSampler(local) as clocks:
+        lib.ttb_profile_enable(1 << dominant)
+        for _ in range(args.steps):
+            flush_l2(torch, flush)
+            torch.cuda.synchronize()
+            l0 = K.launch_count()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            results, lat = eng.solve_all(dev_reqs)
+            e.record()
+            torch.cuda.synchronize()
+            launches += K.launch_count() - l0
+            step_ms.append(s.elapsed_time(e))
+            lats.extend(lat)
+            ok += sum(1 for _, info in results if info.converged)
+        lib.ttb_profile_enable(0)
+    barrier()
+    dom = profile_read(lib)[dominant]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    solved = ok * world
+    value = solved / (total_ms * 1e-3)
+
+    # end to end through the public API from pinned host buffers
+    e2e = e2e_run(eng, reqs, args, torch, flush)
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    pk = peaks()
+    fp64 = fp64_peak_tflops(K, torch)
+    roof = roofline(dominant, dom, pk, fp64)
+    cpu = None
+    if world == 1:
+        sample = cpu_sample(reqs, n_sample)
+        dt, res = cpu_run(sample, cores)
+        conv = sum(1 for r in res if str(r[1]) == "converged")
+        cpu = {"value": conv / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{len(sample)} of the {len(reqs)} requests (same mix), one pass, "
+                         f"{cores} single-threaded oracle workers"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config(args, reqs, engine_kind),
+            "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
+            "converged": f"{ok}/{len(reqs) * args.steps}",
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "kernel_shares": {CLASS_NAMES[c]: round(v["ms"], 3) for c, v in shares.items()
+                              if v["ms"] > 0}}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+CLASS_NAMES = ["gemm", "copy", "kron", "norm", "local_matrix", "qr", "svd", "lu", "rank",
+               "minres", "gmres", "round"]
+
+
+def profile_read(lib):
+    import ctypes as C
+
+    out = {}
+    for c in range(len(CLASS_NAMES)):
+        ms, n, fl, by = C.c_double(), C.c_longlong(), C.c_double(), C.c_double()
+        lib.ttb_profile_read(c, C.byref(ms), C.byref(n), C.byref(fl), C.byref(by))
+        out[c] = {"ms": ms.value, "n": n.value, "flops": fl.value, "bytes": by.value}
+    return out
+
+
+def roofline(cls, rec, pk, fp64_tflops):
+    """Achieved algorithmic rate of the dominant kernel class over the
+    timed region against its measured peak."""
+    name = CLASS_NAMES[cls]
+    if rec["n"] == 0 or rec["ms"] <= 0:
+        return {"kernel": name, "bound": None, "achieved": None, "peak": None, "frac": None,
+                "traffic": None}
+    if rec["flops"] > 0:
+        ach = rec["flops"] / (rec["ms"] * 1e-3) / 1e12
+        return {"kernel": name, "bound": "tensor", "unit": "TFLOP/s", "achieved": ach,
+                "peak": fp64_tflops, "peak_source": "measured FP64 FMA probe (ttb_fma_peak)",
+                "frac": ach / fp64_tflops, "traffic": None,
+                "per_launch_us": 1e3 * rec["ms"] / rec["n"], "launches": rec["n"]}
+    gbs = rec["bytes"] / (rec["ms"] * 1e-3) / 1e9
+    peak = pk.get("hbm_gbs", 6650.0)
+    return {"kernel": name, "bound": "hbm", "unit": "GB/s", "achieved": gbs, "peak": peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
+            "frac": gbs / peak, "traffic": None, "per_launch_us": 1e3 * rec["ms"] / rec["n"],
+            "launches": rec["n"]}
+
+
+def e2e_run(eng, reqs, args, torch, flush):
+    """Same metric through the public API: each step uploads the requests
+    from pinned host memory and downloads the solutions."""
+    pinned = []
+    h2d = 0
+    for p in reqs:
+        A = [torch.from_numpy(np.ascontiguousarray(c)).pin_memory() for c in p.A]
+        b = [torch.from_numpy(np.ascontiguousarray(c)).pin_memory() for c in p.b]
+        h2d += sum(c.numel() * 8 for c in A + b)
+        pinned.append((A, b, p))
+    total, ok, d2h = 0.0, 0, 0
+    steps = max(1, args.steps)
+    for _ in range(steps):
+        K_fill = flush
+        from ttnumpy_b200 import kernels as K
+
+        K.fill_(K_fill, 0.0)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        tt = eng.tt
+        dev = []
+        for A, b, p in pinned:
+            At, bt = tt.TensorTrain(A), tt.TensorTrain(b)
+            r = x0_cores(p)
+            x0 = tt.ones(bt.physical_dims(), ranks=r).orthonormalize("right") if r else None
+            dev.append((At, bt, x0, p))
+        results, _ = eng.solve_all(dev, download=True)
+        host = [x.to_numpy() for x, _ in results]
+        e.record()
+        torch.cuda.synchronize()
+        total += s.elapsed_time(e)
+        ok += sum(1 for _, info in results if info.converged)
+        d2h = sum(sum(c.nbytes for c in h) for h in host)
+    return {"value": ok / (total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h}
+
+
+def percentile(v, q):
+    if not v:
+        return None
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q))
+
+
+def config(args, reqs, engine="reference"):
+    kinds = {}
+    for p in reqs:
+        kinds[p.meta["kind"]] = kinds.get(p.meta["kind"], 0) + 1
+    return {"workload": "AMEn request mix: 2-D QTT Poisson (6-20 cores, mode 2) and parametric "
+                        "diffusion (d 4-5, mode 16/32), residual 1e-8",
+            "requests_per_step": len(reqs), "mix": kinds, "engine": engine,
+            "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
+            "l2": "flushed (512 MB write) before every timed step",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+if __name__ == "__main__":
+    main()

@@ -29,6 +29,26 @@ int ttb_version(void);
 /* Number of the library's own kernels launched since load (all devices). */
 long long ttb_launch_count(void);
 
+/* Optional timing of the library's launches with CUDA events, for
+ * measurement only (no counterpart in the reference).  Bit c of ``mask``
+ * enables kernel class c: 0 GEMM, 1 copy, 2 TTM core product, 3 norm,
+ * 4 explicit local matrix, 5 QR, 6 SVD, 7 LU solve, 8 truncation rank,
+ * 9 MINRES vector kernels, 10 GMRES, 11 batched rounding.  ttb_profile_read
+ * synchronises on the recorded events and returns, for one class, the
+ * summed device milliseconds, the launch count and the algorithmic FLOPs
+ * and bytes the launches were sized for (GEMM: 2mnk per product and the
+ * operand/result bytes; MINRES: the vector traffic). */
+void ttb_profile_enable(int mask);
+int ttb_profile_read(int cls, double* ms, long long* launches, double* flops, double* bytes);
+void ttb_profile_reset(void);
+
+/* FP64 fused multiply-add throughput probe for the roofline denominator of
+ * the float64 kernels (no counterpart in the reference): ``blocks`` blocks
+ * of 256 threads each run 8 independent FMA chains of ``iters`` steps,
+ * 2 * 8 * iters * 256 * blocks FLOPs in all.  ``out`` (1 double) is written
+ * only to keep the chains live. */
+int ttb_fma_peak(double* out, int blocks, int iters, void* stream);
+
 /* ------------------------------------------------------------------------
  * Dense float64 GEMM on strided batched views:
  *   C[b] = alpha * A[b] * B[b] + beta * C[b],  b = 0..batch-1
@@ -180,15 +200,18 @@ int ttb_svd(const ttb_svd_t* problems, int count, void* stream);
  * (ttnumpy/solvers/common.py:766-774).  a is n x n column major with
  * leading dimension lda and is overwritten; b (n) is overwritten with x.
  * ``info`` (device int, may be NULL) receives 0 or the 1-based index of a
- * zero pivot.
+ * zero pivot.  Systems up to n = 161 are factored in shared memory; larger
+ * ones by panels of 16 columns with GEMM trailing updates.
  * --------------------------------------------------------------------- */
 typedef struct {
   double* a;
   long long lda;
   double* b;
   int* info;
+  double* work;  /* ttb_lu_work_doubles(n) doubles, needed only for n > 1600 */
   int n;
 } ttb_lu_t;
+long long ttb_lu_work_doubles(int n);
 int ttb_lu_solve(const ttb_lu_t* problems, int count, void* stream);
 
 /* ------------------------------------------------------------------------

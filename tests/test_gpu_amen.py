@@ -134,11 +134,14 @@ def test_amen_validation_errors(tt):
 
 def test_amen_config1_converges(tt):
     """The 8-D Laplacian (32 points per axis) with a rank-4 right-hand side
-    reaches 1e-8, checked by the host oracle."""
+    reaches 1e-8, checked by the host oracle.  The stagnation test is off:
+    late sweeps improve the residual by factors of 0.85-0.97, so the
+    default 0.9 rule stops the reference itself on some seeds."""
     A_c = P.laplacian_nd(8, 32)
     b_c = P.random_tt([32] * 8, 4, seed=0)
     x, info = tt.amen(tt.TensorTrain(A_c), tt.TensorTrain(b_c), residual_tol=1e-8,
-                      symmetric=True, max_sweeps=20, seed=0, return_info=True)
+                      symmetric=True, max_sweeps=20, seed=0, return_info=True,
+                      stagnation_factor=None)
     assert info.converged, info
     host_res = O.relative_residual(O.Train(A_c), O.Train(b_c), otrain(x))
     assert host_res <= 1.05e-8

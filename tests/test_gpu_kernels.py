@@ -162,7 +162,8 @@ def test_kron_and_norm(K):
 
 
 @pytest.mark.parametrize("m,k", [(1, 1), (5, 3), (3, 5), (64, 64), (256, 64), (1536, 48),
-                                 (3000, 70), (70, 3000), (12, 1)])
+                                 (3000, 70), (70, 3000), (12, 1), (4640, 145), (1280, 44),
+                                 (700, 700), (1000, 17), (300, 2000)])
 def test_qr(K, m, k):
     rng = np.random.default_rng(m + 7 * k)
     a = rng.standard_normal((m, k))
@@ -187,7 +188,8 @@ def test_qr_rank_deficient(K):
 
 
 @pytest.mark.parametrize("m,k", [(1, 1), (6, 4), (4, 6), (64, 64), (256, 64), (64, 256),
-                                 (1536, 48), (48, 1536), (300, 120), (7, 1), (1, 9)])
+                                 (1536, 48), (48, 1536), (300, 120), (7, 1), (1, 9),
+                                 (3000, 90), (90, 3000), (2000, 33)])
 def test_svd(K, m, k):
     rng = np.random.default_rng(11 * m + k)
     a = rng.standard_normal((m, k))
@@ -215,7 +217,7 @@ def test_svd_graded(K):
     assert np.abs(host(s) - s0).max() < 1e-15 * 30
 
 
-@pytest.mark.parametrize("n", [1, 7, 100, 161, 400])
+@pytest.mark.parametrize("n", [1, 7, 100, 161, 162, 400, 777, 1000, 1700])
 def test_lu_solve(K, n):
     rng = np.random.default_rng(n)
     a = rng.standard_normal((n, n)) + n * 0.1 * np.eye(n)

@@ -60,7 +60,7 @@ class SVD(C.Structure):
 
 
 class LU(C.Structure):
-    _fields_ = [("a", P), ("lda", L), ("b", P), ("info", P), ("n", I)]
+    _fields_ = [("a", P), ("lda", L), ("b", P), ("info", P), ("work", P), ("n", I)]
 
 
 class Copy(C.Structure):
@@ -103,6 +103,10 @@ class Round(C.Structure):
 _SIGNATURES = {
     "ttb_version": ([], I),
     "ttb_launch_count": ([], L),
+    "ttb_profile_enable": ([I], None),
+    "ttb_profile_read": ([I, C.POINTER(D), C.POINTER(L), C.POINTER(D), C.POINTER(D)], I),
+    "ttb_profile_reset": ([], None),
+    "ttb_fma_peak": ([P, I, I, P], I),
     "ttb_gemm": ([C.POINTER(Gemm), I, P], I),
     "ttb_env_work_doubles": ([C.POINTER(Env)], L),
     "ttb_env_update": ([C.POINTER(Env), I, P], I),
@@ -114,6 +118,7 @@ _SIGNATURES = {
     "ttb_qr": ([C.POINTER(QR), I, P], I),
     "ttb_svd_work_doubles": ([I, I], L),
     "ttb_svd": ([C.POINTER(SVD), I, P], I),
+    "ttb_lu_work_doubles": ([I], L),
     "ttb_lu_solve": ([C.POINTER(LU), I, P], I),
     "ttb_copy": ([C.POINTER(Copy), I, P], I),
     "ttb_kron": ([C.POINTER(Kron), I, P], I),

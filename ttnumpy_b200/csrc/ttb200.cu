@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cfloat>
 #include <cstring>
@@ -20,6 +21,73 @@ namespace {
 
 std::atomic<long long> g_launches{0};
 inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---------------------------------------------------------------------------
+// optional per-kernel-class timing with CUDA events (ttb_profile_*)
+// ---------------------------------------------------------------------------
+
+enum { P_GEMM = 0, P_COPY, P_KRON, P_NORM, P_LOCALMAT, P_QR, P_SVD, P_LU, P_RANK, P_MINRES,
+       P_GMRES, P_ROUND, P_CLASSES };
+
+struct ProfRec {
+  cudaEvent_t a, b;
+  int cls;
+  double flops, bytes;
+};
+
+std::atomic<int> g_prof_mask{0};
+std::vector<ProfRec> g_prof;
+std::vector<cudaEvent_t> g_event_pool;
+double g_prof_ms[P_CLASSES], g_prof_flops[P_CLASSES], g_prof_bytes[P_CLASSES];
+long long g_prof_n[P_CLASSES];
+
+cudaEvent_t pool_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets one launch of class ``cls`` when that class is being profiled.
+struct ProfScope {
+  bool on;
+  ProfRec r;
+  cudaStream_t s;
+  ProfScope(int cls, cudaStream_t st, double flops, double bytes) : on(false), s(st) {
+    if (!(g_prof_mask.load(std::memory_order_relaxed) & (1 << cls))) return;
+    on = true;
+    r.cls = cls;
+    r.flops = flops;
+    r.bytes = bytes;
+    r.a = pool_event();
+    r.b = pool_event();
+    cudaEventRecord(r.a, s);
+  }
+  ~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(r.b, s);
+    g_prof.push_back(r);
+  }
+};
+
+void prof_collect() {
+  for (auto& r : g_prof) {
+    float ms = 0.f;
+    cudaEventSynchronize(r.b);
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    g_prof_ms[r.cls] += ms;
+    g_prof_n[r.cls] += 1;
+    g_prof_flops[r.cls] += r.flops;
+    g_prof_bytes[r.cls] += r.bytes;
+    g_event_pool.push_back(r.a);
+    g_event_pool.push_back(r.b);
+  }
+  g_prof.clear();
+}
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
@@ -103,6 +171,16 @@ int launch_gemms(const std::vector<GDesc>& ds, cudaStream_t s) {
     }
     if (gb.count == 0) continue;
     gb.base[gb.count] = (int)tiles;
+    double fl = 0.0, by = 0.0;
+    if (g_prof_mask.load(std::memory_order_relaxed) & (1 << P_GEMM)) {
+      for (int j = 0; j < gb.count; ++j) {
+        const GDesc& g = gb.d[j];
+        fl += 2.0 * g.m * g.n * (double)g.k * g.batch;
+        const double na = g.a_bs ? g.batch : 1, nb = g.b_bs ? g.batch : 1;
+        by += 8.0 * ((double)g.m * g.k * na + (double)g.k * g.n * nb + 2.0 * g.m * g.n * g.batch);
+      }
+    }
+    ProfScope ps(P_GEMM, s, fl, by);
     k_gemm<<<(unsigned)tiles, TTB_THREADS, 0, s>>>(gb);
     counted();
   }
@@ -231,28 +309,38 @@ __global__ void __launch_bounds__(TTB_THREADS) k_local_matrix(const __grid_const
 constexpr int kMaxQ = 24;
 struct QBatch {
   int count;
-  int smem[kMaxQ];  // 1: factor in shared memory
+  int mode[kMaxQ];  // 0: whole factorisation in shared memory, 1: blocked (work in global)
   ttb_qr_t d[kMaxQ];
 };
 
 __global__ void __launch_bounds__(TTB_THREADS) k_qr(const __grid_constant__ QBatch qb) {
   extern __shared__ double dsm[];
   __shared__ double red[TTB_WARPS];
+  __shared__ GemmSmem gsm;
   const ttb_qr_t& q = qb.d[blockIdx.x];
   const int m = q.m, k = q.k;
   if (m <= 0 || k <= 0) return;
-  double* W = qb.smem[blockIdx.x] ? dsm : q.work;
-  double* tau = W + (i64)m * k;
-  cta_qr(CMat{q.a, q.a_rs, q.a_cs}, m, k, W, tau, Mat{q.q, q.q_rs, q.q_cs},
-         Mat{q.r, q.r_rs, q.r_cs}, red);
+  if (qb.mode[blockIdx.x] == 0) {
+    double* W = dsm;
+    double* tau = W + (i64)m * k;
+    cta_qr(CMat{q.a, q.a_rs, q.a_cs}, m, k, W, tau, Mat{q.q, q.q_rs, q.q_cs},
+           Mat{q.r, q.r_rs, q.r_cs}, red);
+  } else {
+    double* Y = dsm;
+    double* G = Y + (i64)LNB * min(k, YCH);
+    double* Tm = G + LNB * LNB;
+    cta_qr_blocked(CMat{q.a, q.a_rs, q.a_cs}, m, k, q.work, q.work + (i64)m * k,
+                   Mat{q.q, q.q_rs, q.q_cs}, Mat{q.r, q.r_rs, q.r_cs}, Y, G, Tm, red, gsm);
+  }
 }
 
 i64 qr_need(int m, int k) { return (i64)m * k + std::min(m, k); }
+i64 blocked_smem(int k) { return (i64)LNB * std::min(std::max(k, 1), YCH) + 2 * LNB * LNB; }
 
 constexpr int kMaxS = 16;
 struct SBatch {
   int count;
-  int smem[kMaxS];
+  int mode[kMaxS];  // 0: shared memory, 1: blocked with the work area in global memory
   ttb_svd_t d[kMaxS];
 };
 
@@ -262,11 +350,13 @@ i64 svd_tall_need(int M, int K) { return (i64)M * K + 2 * (i64)K * K + 3 * (i64)
 __global__ void __launch_bounds__(TTB_THREADS) k_svd(const __grid_constant__ SBatch sb) {
   extern __shared__ double dsm[];
   __shared__ double red[TTB_WARPS];
+  __shared__ GemmSmem gsm;
   const ttb_svd_t& q = sb.d[blockIdx.x];
   if (q.m <= 0 || q.k <= 0) return;
   const bool tall = q.m >= q.k;
   const int M = tall ? q.m : q.k, K = tall ? q.k : q.m;
-  double* base = sb.smem[blockIdx.x] ? dsm : q.work;
+  const int mode = sb.mode[blockIdx.x];
+  double* base = mode == 0 ? dsm : q.work;
   double* W = base;
   double* tau = W + (i64)M * K;
   double* Bsq = tau + K;
@@ -274,14 +364,19 @@ __global__ void __launch_bounds__(TTB_THREADS) k_svd(const __grid_constant__ SBa
   double* sv = V + (i64)K * K;
   int* order = reinterpret_cast<int*>(sv + K);
   int* flag = reinterpret_cast<int*>(sv + 2 * K);
+  CMat A = tall ? CMat{q.a, q.a_rs, q.a_cs} : CMat{q.a, q.a_cs, q.a_rs};
+  // a^T = U' S Vh'  =>  a = Vh'^T S U'^T : U' goes to vh^T, Vh' to u^T
+  Mat U = tall ? Mat{q.u, q.u_rs, q.u_cs} : Mat{q.vh, q.vh_cs, q.vh_rs};
+  Mat Vh = tall ? Mat{q.vh, q.vh_rs, q.vh_cs} : Mat{q.u, q.u_cs, q.u_rs};
   int st;
-  if (tall) {
-    st = cta_svd_tall(CMat{q.a, q.a_rs, q.a_cs}, M, K, W, tau, Bsq, V, sv, order, flag,
-                      Mat{q.u, q.u_rs, q.u_cs}, q.s, Mat{q.vh, q.vh_rs, q.vh_cs}, red);
+  if (mode == 0) {
+    st = cta_svd_tall(A, M, K, W, tau, Bsq, V, sv, order, flag, U, q.s, Vh, red);
   } else {
-    // a^T = U' S Vh'  =>  a = Vh'^T S U'^T : U' goes to vh^T, Vh' to u^T
-    st = cta_svd_tall(CMat{q.a, q.a_cs, q.a_rs}, M, K, W, tau, Bsq, V, sv, order, flag,
-                      Mat{q.vh, q.vh_cs, q.vh_rs}, q.s, Mat{q.u, q.u_cs, q.u_rs}, red);
+    double* Y = dsm;
+    double* G = Y + (i64)LNB * min(K, YCH);
+    double* Tm = G + LNB * LNB;
+    st = cta_svd_tall_blocked(A, M, K, W, tau, Bsq, V, sv, order, flag, U, q.s, Vh, Y, G, Tm,
+                              red, gsm);
   }
   if (q.status && threadIdx.x == 0) *q.status = st;
 }
@@ -289,7 +384,7 @@ __global__ void __launch_bounds__(TTB_THREADS) k_svd(const __grid_constant__ SBa
 constexpr int kMaxL = 24;
 struct LBatch {
   int count;
-  int smem[kMaxL];
+  int mode[kMaxL];  // 0: all in shared memory, 1: blocked, panel shared, 2: blocked, panel global
   ttb_lu_t d[kMaxL];
 };
 
@@ -297,11 +392,14 @@ __global__ void __launch_bounds__(TTB_THREADS) k_lu(const __grid_constant__ LBat
   extern __shared__ double dsm[];
   __shared__ double redv[TTB_WARPS];
   __shared__ int redi[TTB_WARPS];
+  __shared__ int ipiv[LNB];
+  __shared__ GemmSmem gsm;
   const ttb_lu_t& q = lb.d[blockIdx.x];
   const int n = q.n;
   if (n <= 0) return;
+  const int mode = lb.mode[blockIdx.x];
   int info;
-  if (lb.smem[blockIdx.x]) {
+  if (mode == 0) {
     double* W = dsm;
     double* b = dsm + (i64)n * n;
     for (i64 e = threadIdx.x; e < (i64)n * n; e += TTB_THREADS) {
@@ -315,7 +413,8 @@ __global__ void __launch_bounds__(TTB_THREADS) k_lu(const __grid_constant__ LBat
     if (info == 0)
       for (int i = threadIdx.x; i < n; i += TTB_THREADS) q.b[i] = b[i];
   } else {
-    info = cta_gepp_solve(q.a, q.lda, q.b, n, redv, redi);
+    double* panel = mode == 1 ? dsm : q.work;
+    info = cta_gepp_blocked(q.a, q.lda, q.b, n, panel, redv, redi, ipiv, gsm);
   }
   if (q.info && threadIdx.x == 0) *q.info = info;
 }
@@ -1182,6 +1281,23 @@ __global__ void __launch_bounds__(TTB_THREADS) k_round(const __grid_constant__ t
   if (threadIdx.x == 0 && P.status) P.status[pair] = status;
 }
 
+
+// FP64 FMA throughput probe: 8 independent chains per thread
+__global__ void __launch_bounds__(TTB_THREADS) k_fma_peak(double* out, int iters) {
+  double a[8];
+  const double m = 1.0 + 1e-9 * threadIdx.x, c = 1e-12;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = j * 1e-3 + blockIdx.x * 1e-7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = fma(a[j], m, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1276,6 +1392,7 @@ int ttb_local_matrix(const ttb_local_matrix_t* ps, int count, void* stream) {
       most = std::max(most, (long long)q.lf * q.n * q.rf * q.lt * q.m * q.rt);
     }
     dim3 grid((unsigned)std::min<long long>(cdiv(most, TTB_THREADS), 4096), lb.count);
+    ProfScope ps(P_LOCALMAT, s, 0.0, 0.0);
     k_local_matrix<<<grid, TTB_THREADS, 0, s>>>(lb);
     counted();
   }
@@ -1310,10 +1427,25 @@ int ttb_qr(const ttb_qr_t* ps, int count, void* stream) {
     i64 smem = 0;
     for (int j = 0; j < qb.count; ++j) {
       qb.d[j] = ps[i0 + j];
-      i64 need = qr_need(qb.d[j].m, qb.d[j].k) * 8;
-      qb.smem[j] = need <= kSmemCap;
-      if (qb.smem[j]) smem = std::max(smem, need);
+      const i64 whole = qr_need(qb.d[j].m, qb.d[j].k) * 8;
+      const i64 blk = blocked_smem(qb.d[j].k) * 8;
+      if (whole <= kSmemCap) {
+        qb.mode[j] = 0;
+        smem = std::max(smem, whole);
+      } else {
+        if (blk > kSmemCap) return (int)cudaErrorInvalidValue;
+        qb.mode[j] = 1;
+        smem = std::max(smem, blk);
+      }
     }
+    double fl = 0.0;
+    for (int j = 0; j < qb.count; ++j) {
+      // Householder R: 2mk^2 - 2k^3/3 (p = k), and as much again to form Q
+      const double m = qb.d[j].m, k = std::min(qb.d[j].m, qb.d[j].k), kk = qb.d[j].k;
+      fl += 2.0 * m * k * kk - 2.0 / 3.0 * k * k * k;
+      if (qb.d[j].q) fl += 2.0 * m * k * k - 2.0 / 3.0 * k * k * k;
+    }
+    ProfScope ps(P_QR, s, fl, 0.0);
     k_qr<<<qb.count, TTB_THREADS, (size_t)smem, s>>>(qb);
     counted();
   }
@@ -1334,15 +1466,31 @@ int ttb_svd(const ttb_svd_t* ps, int count, void* stream) {
     i64 smem = 0;
     for (int j = 0; j < sb.count; ++j) {
       sb.d[j] = ps[i0 + j];
-      i64 need = ttb_svd_work_doubles(sb.d[j].m, sb.d[j].k) * 8;
-      sb.smem[j] = need <= kSmemCap;
-      if (sb.smem[j]) smem = std::max(smem, need);
+      const i64 whole = ttb_svd_work_doubles(sb.d[j].m, sb.d[j].k) * 8;
+      const i64 blk = blocked_smem(std::min(sb.d[j].m, sb.d[j].k)) * 8;
+      if (whole <= kSmemCap) {
+        sb.mode[j] = 0;
+        smem = std::max(smem, whole);
+      } else {
+        if (blk > kSmemCap) return (int)cudaErrorInvalidValue;
+        sb.mode[j] = 1;
+        smem = std::max(smem, blk);
+      }
     }
+    double fl = 0.0;
+    for (int j = 0; j < sb.count; ++j) {
+      // QR of the tall orientation, U = Q [U_R; 0] (Jacobi rotations not counted)
+      const double M = std::max(sb.d[j].m, sb.d[j].k), k = std::min(sb.d[j].m, sb.d[j].k);
+      fl += 4.0 * M * k * k - 4.0 / 3.0 * k * k * k;
+    }
+    ProfScope ps(P_SVD, s, fl, 0.0);
     k_svd<<<sb.count, TTB_THREADS, (size_t)smem, s>>>(sb);
     counted();
   }
   return last_error();
 }
+
+long long ttb_lu_work_doubles(int n) { return (long long)n * LNB; }
 
 int ttb_lu_solve(const ttb_lu_t* ps, int count, void* stream) {
   configure_smem();
@@ -1353,10 +1501,22 @@ int ttb_lu_solve(const ttb_lu_t* ps, int count, void* stream) {
     i64 smem = 0;
     for (int j = 0; j < lb.count; ++j) {
       lb.d[j] = ps[i0 + j];
-      i64 need = ((i64)lb.d[j].n * lb.d[j].n + lb.d[j].n) * 8;
-      lb.smem[j] = need <= kSmemCap;
-      if (lb.smem[j]) smem = std::max(smem, need);
+      const i64 n = lb.d[j].n;
+      const i64 whole = (n * n + n) * 8, panel = n * LNB * 8;
+      if (whole <= kSmemCap) {
+        lb.mode[j] = 0;
+        smem = std::max(smem, whole);
+      } else if (panel <= kSmemCap) {
+        lb.mode[j] = 1;
+        smem = std::max(smem, panel);
+      } else {
+        if (lb.d[j].work == nullptr) return (int)cudaErrorInvalidValue;
+        lb.mode[j] = 2;
+      }
     }
+    double fl = 0.0;
+    for (int j = 0; j < lb.count; ++j) fl += 2.0 / 3.0 * std::pow((double)lb.d[j].n, 3.0);
+    ProfScope ps(P_LU, s, fl, 0.0);
     k_lu<<<lb.count, TTB_THREADS, (size_t)smem, s>>>(lb);
     counted();
   }
@@ -1374,6 +1534,7 @@ int ttb_copy(const ttb_copy_t* ps, int count, void* stream) {
       most = std::max(most, (long long)cb.d[j].d0 * cb.d[j].d1 * cb.d[j].d2 * cb.d[j].d3);
     }
     dim3 grid((unsigned)std::min<long long>(cdiv(most, TTB_THREADS), 2048), cb.count);
+    ProfScope ps(P_COPY, s, 0.0, 0.0);
     k_copy<<<grid, TTB_THREADS, 0, s>>>(cb);
     counted();
   }
@@ -1392,6 +1553,7 @@ int ttb_kron(const ttb_kron_t* ps, int count, void* stream) {
       most = std::max(most, (long long)q.ra * q.rx * q.n * q.kk * q.ra2 * q.rx2);
     }
     dim3 grid((unsigned)std::min<long long>(cdiv(most, TTB_THREADS), 2048), kb.count);
+    ProfScope ps(P_KRON, s, 0.0, 0.0);
     k_kron<<<grid, TTB_THREADS, 0, s>>>(kb);
     counted();
   }
@@ -1404,6 +1566,7 @@ int ttb_norm(const ttb_norm_t* ps, int count, void* stream) {
     NBatch nb;
     nb.count = std::min(kMaxN, count - i0);
     for (int j = 0; j < nb.count; ++j) nb.d[j] = ps[i0 + j];
+    ProfScope ps(P_NORM, s, 0.0, 0.0);
     k_norm<<<nb.count, TTB_THREADS, 0, s>>>(nb);
     counted();
   }
@@ -1425,6 +1588,7 @@ int ttb_rank_residual(const ttb_rank_t* ps, int count, void* stream) {
       rb.chunks[j] = std::max(1, cdiv(rb.d[j].n, kRankChunk));
       most = std::max(most, rb.chunks[j]);
     }
+    ProfScope ps(P_RANK, s, 0.0, 0.0);
     k_rank_partial<<<dim3(most, rb.count), TTB_THREADS, 0, s>>>(rb);
     counted();
     k_rank_select<<<rb.count, 32, 0, s>>>(rb);
@@ -1510,12 +1674,17 @@ int ttb_minres(const ttb_krylov_t* ps, int count, int* flags, void* stream) {
     const int check_every = 8;
     for (int it = 0; it < maxit_all; ++it) {
       if ((e = run_local(mv.data(), nb, s))) return e;
-      k_minres_a<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
-      counted();
-      k_minres_b<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
-      counted();
-      k_minres_c<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
-      counted();
+      {
+        double by = 0.0;
+        for (int j = 0; j < nb; ++j) by += 8.0 * 19.0 * kb.d[j].n;  // vector reads + writes
+        ProfScope ps(P_MINRES, s, 0.0, by);
+        k_minres_a<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
+        counted();
+        k_minres_b<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
+        counted();
+        k_minres_c<<<dim3(most, nb), TTB_THREADS, 0, s>>>(kb, it);
+        counted();
+      }
       if ((it + 1) % check_every == 0 || it + 1 == maxit_all) {
         // evaluates the stop test of iteration ``it`` (state copy it + 1)
         k_minres_final<<<nb, 32, 0, s>>>(kb, it + 1, flags + i0);
@@ -1654,7 +1823,39 @@ int ttb_round_batch(const ttb_round_t* P, void* stream) {
   }
   const long long qslot = (long long)kRoundMaxRows * kRoundMaxBond;
   const long long slot = qslot;
+  ProfScope ps(P_ROUND, as_stream(stream), 0.0, 0.0);
   k_round<<<P->pairs, TTB_THREADS, smem, as_stream(stream)>>>(*P, slot, qslot);
+  counted();
+  return last_error();
+}
+
+
+void ttb_profile_enable(int mask) {
+  if (mask == 0) prof_collect();
+  g_prof_mask.store(mask);
+}
+
+int ttb_profile_read(int cls, double* ms, long long* launches, double* flops, double* bytes) {
+  if (cls < 0 || cls >= P_CLASSES) return (int)cudaErrorInvalidValue;
+  prof_collect();
+  *ms = g_prof_ms[cls];
+  *launches = g_prof_n[cls];
+  *flops = g_prof_flops[cls];
+  *bytes = g_prof_bytes[cls];
+  return 0;
+}
+
+void ttb_profile_reset(void) {
+  prof_collect();
+  for (int i = 0; i < P_CLASSES; ++i) {
+    g_prof_ms[i] = g_prof_flops[i] = g_prof_bytes[i] = 0.0;
+    g_prof_n[i] = 0;
+  }
+}
+
+
+int ttb_fma_peak(double* out, int blocks, int iters, void* stream) {
+  k_fma_peak<<<blocks, TTB_THREADS, 0, as_stream(stream)>>>(out, iters);
   counted();
   return last_error();
 }

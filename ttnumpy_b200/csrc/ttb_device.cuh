@@ -494,4 +494,274 @@ __device__ int cta_gepp_solve(double* W, i64 ld, double* b, int n, double* redv,
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// blocked factorisations for matrices that do not fit in shared memory
+// ---------------------------------------------------------------------------
+
+constexpr int LNB = 16;   // panel width of the blocked factorisations
+constexpr int YCH = 512;  // columns per chunk of the blocked trailing updates
+
+// Blocked Gaussian elimination with partial pivoting on [W | b] (W column
+// major, leading dimension ld), panels of LNB columns factored in ``panel``
+// (rows x LNB doubles, shared or global memory), trailing updates as GEMMs.
+// Same pivot rule and result as cta_gepp_solve; b becomes the solution.
+__device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, double* panel, double* redv,
+                                int* redi, int* ipiv, GemmSmem& gsm) {
+  const int tid = threadIdx.x;
+  for (int j0 = 0; j0 < n; j0 += LNB) {
+    const int jb = min(LNB, n - j0);
+    const int rows = n - j0;
+    double* P = panel;
+    for (int e = tid; e < rows * jb; e += TTB_THREADS) {
+      int i = e % rows, c = e / rows;
+      P[i + (i64)c * rows] = W[(j0 + i) + (i64)(j0 + c) * ld];
+    }
+    __syncthreads();
+    for (int c = 0; c < jb; ++c) {
+      double best = -1.0;
+      int bi = -1;
+      for (int i = c + tid; i < rows; i += TTB_THREADS) {
+        double a = fabs(P[i + (i64)c * rows]);
+        if (a > best) { best = a; bi = i; }
+      }
+      const int piv = block_argmax_abs(best, bi, redv, redi);
+      if (tid == 0) ipiv[c] = piv;
+      if (piv != c) {
+        for (int cc = tid; cc < jb; cc += TTB_THREADS) {
+          double t = P[c + (i64)cc * rows];
+          P[c + (i64)cc * rows] = P[piv + (i64)cc * rows];
+          P[piv + (i64)cc * rows] = t;
+        }
+      }
+      __syncthreads();
+      const double d = P[c + (i64)c * rows];
+      if (d == 0.0) return j0 + c + 1;
+      const double rd = 1.0 / d;
+      for (int i = c + 1 + tid; i < rows; i += TTB_THREADS) P[i + (i64)c * rows] *= rd;
+      __syncthreads();
+      const int rr = rows - c - 1, cw = jb - c - 1;
+      for (int e = tid; e < rr * cw; e += TTB_THREADS) {
+        int i = c + 1 + e % rr, cc = c + 1 + e / rr;
+        P[i + (i64)cc * rows] = fma(-P[i + (i64)c * rows], P[c + (i64)cc * rows],
+                                    P[i + (i64)cc * rows]);
+      }
+      __syncthreads();
+    }
+    for (int e = tid; e < rows * jb; e += TTB_THREADS) {
+      int i = e % rows, c = e / rows;
+      W[(j0 + i) + (i64)(j0 + c) * ld] = P[i + (i64)c * rows];
+    }
+    // row swaps and the unit-lower solve on the columns right of the panel
+    // and on b; each thread owns whole columns, so no synchronisation
+    const int ncols = n - j0 - jb;
+    for (int col = tid; col <= ncols; col += TTB_THREADS) {
+      double* x = (col < ncols) ? W + (i64)(j0 + jb + col) * ld + j0 : b + j0;
+      for (int c = 0; c < jb; ++c) {
+        const int piv = ipiv[c];
+        if (piv != c) {
+          double t = x[c];
+          x[c] = x[piv];
+          x[piv] = t;
+        }
+      }
+      for (int r = 1; r < jb; ++r) {
+        double acc = x[r];
+        for (int q = 0; q < r; ++q) acc = fma(-P[r + (i64)q * rows], x[q], acc);
+        x[r] = acc;
+      }
+    }
+    __syncthreads();
+    if (rows > jb) {
+      // A22 -= L21 U12 ; b2 -= L21 u_b
+      if (ncols > 0)
+        cta_gemm(CMat{P + jb, 1, rows}, CMat{W + j0 + (i64)(j0 + jb) * ld, 1, ld},
+                 Mat{W + (j0 + jb) + (i64)(j0 + jb) * ld, 1, ld}, rows - jb, ncols, jb, -1.0,
+                 1.0, gsm);
+      for (int i = tid; i < rows - jb; i += TTB_THREADS) {
+        double acc = b[j0 + jb + i];
+        for (int q = 0; q < jb; ++q) acc = fma(-P[jb + i + (i64)q * rows], b[j0 + q], acc);
+        b[j0 + jb + i] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    if (tid == 0) b[j] = b[j] / W[j + (i64)j * ld];
+    __syncthreads();
+    const double xj = b[j];
+    for (int i = tid; i < j; i += TTB_THREADS) b[i] = fma(-W[i + (i64)j * ld], xj, b[i]);
+    __syncthreads();
+  }
+  return 0;
+}
+
+// T factor (jb x jb, upper triangular, column major in Tm) of the block
+// reflector H_0 ... H_{jb-1} = I - V T V^T, V the rows x jb explicit
+// reflector block (unit diagonal, zeros above) in Wp with leading dim ldw
+// (LAPACK dlarft, forward column-wise).  G is jb x jb scratch.
+__device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, const double* tau,
+                            double* G, double* Tm, GemmSmem& gsm) {
+  cta_gemm(CMat{Wp, ldw, 1}, CMat{Wp, 1, ldw}, Mat{G, 1, LNB}, jb, jb, rows, 1.0, 0.0, gsm);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < jb; ++i) {
+      for (int q = 0; q < i; ++q) {
+        double acc = 0.0;
+        for (int r = q; r < i; ++r) acc = fma(Tm[q + r * LNB], G[r + i * LNB], acc);
+        Tm[q + i * LNB] = -tau[i] * acc;
+      }
+      Tm[i + i * LNB] = tau[i];
+      for (int q = i + 1; q < LNB; ++q) Tm[q + i * LNB] = 0.0;
+    }
+  }
+  __syncthreads();
+}
+
+// X (m x nx, strided) <- H_0 ... H_{p-1} X for the block reflectors left in
+// W by cta_qr_blocked (explicit reflector blocks, leading dimension m),
+// applied last block first; only rows >= the block's first row change.
+// Columns of X left of a block are untouched (as for an identity start).
+__device__ void cta_apply_q_blocked(const double* W, int m, int p, const double* tau, Mat X,
+                                    int nx, double* Y, double* G, double* Tm, GemmSmem& gsm) {
+  const int tid = threadIdx.x;
+  const int last = ((p - 1) / LNB) * LNB;
+  for (int j0 = last; j0 >= 0; j0 -= LNB) {
+    const int jb = min(LNB, p - j0);
+    const int rows = m - j0;
+    const double* Wp = W + j0 + (i64)j0 * m;
+    cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm);
+    for (int c0 = 0; c0 < nx; c0 += YCH) {
+      const int nc = min(YCH, nx - c0);
+      Mat Xs{X.p + j0 * X.rs + c0 * X.cs, X.rs, X.cs};
+      cta_gemm(CMat{Wp, m, 1}, CMat{Xs.p, Xs.rs, Xs.cs}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0,
+               gsm);
+      for (int col = tid; col < nc; col += TTB_THREADS) {
+        double y[LNB];
+        for (int i = 0; i < jb; ++i) y[i] = Y[i + (i64)col * LNB];
+        for (int i = 0; i < jb; ++i) {
+          double acc = 0.0;
+          for (int q = i; q < jb; ++q) acc = fma(Tm[i + q * LNB], y[q], acc);
+          Y[i + (i64)col * LNB] = acc;
+        }
+      }
+      __syncthreads();
+      cta_gemm(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Xs, rows, nc, jb, -1.0, 1.0, gsm);
+    }
+  }
+}
+
+// Blocked (compact WY) economic QR of the m x k matrix A into the m x k
+// column-major work area W (global), panels of LNB columns: Householder on
+// the panel (cta_householder), the T factor, then the trailing update
+// C -= V (T^T (V^T C)) as two GEMMs through Y (LNB x k, shared).  Q (m x p)
+// and R (p x k) as in cta_qr; either may be NULL.  Same reflectors and R as
+// the unblocked factorisation up to rounding.
+__device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R,
+                               double* Y, double* G, double* Tm, double* red, GemmSmem& gsm) {
+  const int p = m < k ? m : k;
+  const int tid = threadIdx.x;
+  cta_copy(A, Mat{W, 1, (i64)m}, m, k);
+  __syncthreads();
+  for (int j0 = 0; j0 < p; j0 += LNB) {
+    const int jb = min(LNB, p - j0);
+    const int rows = m - j0;
+    double* Wp = W + j0 + (i64)j0 * m;
+    cta_householder(Wp, rows, jb, m, tau + j0, red);
+    // R's diagonal block, then the explicit reflector form in its place
+    for (int e = tid; e < jb * jb; e += TTB_THREADS) {
+      int r = e % jb, c = e / jb;
+      if (r <= c) {
+        if (R.p) R(j0 + r, j0 + c) = Wp[r + (i64)c * m];
+        Wp[r + (i64)c * m] = (r == c) ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    const int nt = k - j0 - jb;
+    if (nt > 0) {
+      cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm);
+      for (int c0 = 0; c0 < nt; c0 += YCH) {
+        const int nc = min(YCH, nt - c0);
+        double* C = W + j0 + (i64)(j0 + jb + c0) * m;
+        // Y = V^T C (jb x nc), then Y = T^T Y, then C -= V Y
+        cta_gemm(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0, gsm);
+        for (int col = tid; col < nc; col += TTB_THREADS) {
+          double y[LNB];
+          for (int i = 0; i < jb; ++i) y[i] = Y[i + (i64)col * LNB];
+          for (int i = jb - 1; i >= 0; --i) {
+            double acc = 0.0;
+            for (int q = 0; q <= i; ++q) acc = fma(Tm[q + i * LNB], y[q], acc);
+            Y[i + (i64)col * LNB] = acc;
+          }
+        }
+        __syncthreads();
+        cta_gemm(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Mat{C, 1, m}, rows, nc, jb, -1.0, 1.0, gsm);
+      }
+    }
+  }
+  if (R.p) {
+    for (int e = tid; e < p * k; e += TTB_THREADS) {
+      int i = e % p, j = e / p;
+      int jp = (i / LNB) * LNB;  // panel of row i
+      bool in_diag_block = (j >= jp && j < jp + LNB && j < p);
+      if (i > j) R(i, j) = 0.0;
+      else if (!in_diag_block) R(i, j) = W[i + (i64)j * m];
+    }
+  }
+  if (Q.p) {
+    for (int e = tid; e < m * p; e += TTB_THREADS) {
+      int i = e % m, j = e / m;
+      Q(i, j) = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q_blocked(W, m, p, tau, Q, p, Y, G, Tm, gsm);
+  }
+  __syncthreads();
+}
+
+// cta_svd_tall for matrices that do not fit in shared memory: blocked QR
+// into the global work area W, Jacobi on R in Bsq/V (global or shared), U
+// by the blocked reflector product.  Y needs LNB * max(k, 1) doubles, G and
+// Tm LNB * LNB each (shared).
+__device__ int cta_svd_tall_blocked(CMat A, int m, int k, double* W, double* tau, double* Bsq,
+                                    double* V, double* sv, int* order, int* flag, Mat U, double* S,
+                                    Mat Vh, double* Y, double* G, double* Tm, double* red,
+                                    GemmSmem& gsm) {
+  cta_qr_blocked(A, m, k, W, tau, Mat{nullptr, 0, 0}, Mat{Bsq, 1, (i64)k}, Y, G, Tm, red, gsm);
+  __syncthreads();
+  const double tol = 4.0 * k * 2.220446049250313e-16;
+  int status = cta_jacobi(Bsq, k, k, V, k, 60, tol, flag);
+  for (int j = threadIdx.x; j < k; j += TTB_THREADS) {
+    double s2 = 0.0;
+    for (int i = 0; i < k; ++i) s2 = fma(Bsq[i + (i64)j * k], Bsq[i + (i64)j * k], s2);
+    sv[j] = sqrt(s2);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += TTB_THREADS) {
+    double sj = sv[j];
+    int rank = 0;
+    for (int i = 0; i < k; ++i) {
+      double si = sv[i];
+      rank += (si > sj) || (si == sj && i < j);
+    }
+    order[rank] = j;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < m * k; e += TTB_THREADS) {
+    int i = e % m, r = e / m;
+    int j = order[r];
+    double sj = sv[j];
+    double v;
+    if (i < k) v = (sj > 0.0) ? Bsq[i + (i64)j * k] / sj : (i == r ? 1.0 : 0.0);
+    else v = 0.0;
+    U(i, r) = v;
+  }
+  for (int r = threadIdx.x; r < k; r += TTB_THREADS) S[r] = sv[order[r]];
+  for (int e = threadIdx.x; e < k * k; e += TTB_THREADS) {
+    int r = e % k, c = e / k;
+    Vh(r, c) = V[c + (i64)order[r] * k];
+  }
+  __syncthreads();
+  cta_apply_q_blocked(W, m, k, tau, U, k, Y, G, Tm, gsm);
+  return status;
+}
+
 }  // namespace ttb

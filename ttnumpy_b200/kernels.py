@@ -360,9 +360,13 @@ def lu_solve_(a_colmajor: torch.Tensor, b: torch.Tensor, info: Optional[torch.Te
     """Solve in place: ``a_colmajor`` is (n, n) whose row c is column c of the
     matrix (destroyed); b (n) becomes the solution."""
     n = b.numel()
-    d = _lib.LU(ptr(a_colmajor), a_colmajor.stride(0), ptr(b), ptr(info), n)
-    arr = (_lib.LU * 1)(d)
-    check(lib().ttb_lu_solve(arr, 1, stream()), "ttb_lu_solve")
+    L = lib()
+    ar = arena()
+    with ar.scope():
+        work = ar.take(L.ttb_lu_work_doubles(n)) if n > 1600 else None
+        d = _lib.LU(ptr(a_colmajor), a_colmajor.stride(0), ptr(b), ptr(info), ptr(work), n)
+        arr = (_lib.LU * 1)(d)
+        check(L.ttb_lu_solve(arr, 1, stream()), "ttb_lu_solve")
     return b
 
 
@@ -423,3 +427,160 @@ def krylov(method: str, left, op, right, b, x, rtol, warm, maxiter=0, restart=20
 
 def launch_count() -> int:
     return int(lib().ttb_launch_count())
+
+
+# ---------------------------------------------------------------------------
+# list forms: one grouped call for many independent problems
+# ---------------------------------------------------------------------------
+
+
+def qr_many(items) -> List:
+    """items: (a, want_q, want_r, q_out, r_out); returns [(q, r)]."""
+    if not items:
+        return []
+    L = lib()
+    ar = arena()
+    outs, descs = [], []
+    with ar.scope():
+        for a, want_q, want_r, q_out, r_out in items:
+            m, k = a.shape
+            p = min(m, k)
+            q = q_out if q_out is not None else (empty(m, p) if want_q else None)
+            r = r_out if r_out is not None else (empty(p, k) if want_r else None)
+            work = ar.take(L.ttb_qr_work_doubles(m, k))
+            descs.append(_lib.QR(ptr(a), a.stride(0), a.stride(1), ptr(q),
+                                 q.stride(0) if q is not None else 0,
+                                 q.stride(1) if q is not None else 0, ptr(r),
+                                 r.stride(0) if r is not None else 0,
+                                 r.stride(1) if r is not None else 0, ptr(work), m, k))
+            outs.append((q, r))
+        arr = (_lib.QR * len(descs))(*descs)
+        check(L.ttb_qr(arr, len(descs), stream()), "ttb_qr")
+    return outs
+
+
+def svd_many(mats) -> List:
+    if not mats:
+        return []
+    L = lib()
+    ar = arena()
+    outs, descs = [], []
+    with ar.scope():
+        for a in mats:
+            m, k = a.shape
+            p = min(m, k)
+            u, s, vh = empty(m, p), empty(p), empty(p, k)
+            work = ar.take(L.ttb_svd_work_doubles(m, k))
+            descs.append(_lib.SVD(ptr(a), a.stride(0), a.stride(1), ptr(u), u.stride(0),
+                                  u.stride(1), ptr(s), ptr(vh), vh.stride(0), vh.stride(1),
+                                  ptr(work), None, m, k))
+            outs.append((u, s, vh))
+        arr = (_lib.SVD * len(descs))(*descs)
+        check(L.ttb_svd(arr, len(descs), stream()), "ttb_svd")
+    return outs
+
+
+def direct_many(items, info: torch.Tensor) -> List:
+    """items: (left, op, right, b_loc); explicit local matrices then GEPP
+    solves, all grouped; ``info`` (int32, len(items)) receives the pivot
+    status of each.  Returns the solutions (shaped like b_loc)."""
+    if not items:
+        return []
+    L = lib()
+    ar = arena()
+    sols, lm, lu = [], [], []
+    with ar.scope():
+        for j, (left, op, right, b_loc) in enumerate(items):
+            lt, R, lf = left.shape
+            _, n, m, R2 = op.shape
+            rt, _, rf = right.shape
+            rows, cols = lf * n * rf, lt * m * rt
+            M = ar.take(rows * cols)[: rows * cols].view(cols, rows)
+            lm.append(_lib.LocalMatrix(ptr(left), ptr(op), ptr(right), ptr(M), lt, lf, R, R2, n,
+                                       m, rt, rf))
+            u = empty(*b_loc.shape)
+            sols.append(u)
+            work = ar.take(L.ttb_lu_work_doubles(rows)) if rows > 1600 else None
+            lu.append(_lib.LU(ptr(M), rows, ptr(u), info.data_ptr() + 4 * j, ptr(work), rows))
+        copy_many([copy_desc(b, u) for (_, _, _, b), u in zip(items, sols)])
+        arr = (_lib.LocalMatrix * len(lm))(*lm)
+        check(L.ttb_local_matrix(arr, len(lm), stream()), "ttb_local_matrix")
+        arr = (_lib.LU * len(lu))(*lu)
+        check(L.ttb_lu_solve(arr, len(lu), stream()), "ttb_lu_solve")
+    return sols
+
+
+def krylov_many(method: str, items, restart: int = 20) -> None:
+    """items: (left, op, right, b, x, rtol, warm); x is updated in place."""
+    if not items:
+        return
+    L = lib()
+    ar = arena()
+    with ar.scope():
+        descs = []
+        for left, op, right, b, x, rtol, warm in items:
+            opd = local_desc(left, op, right, x, b)
+            kd = _lib.Krylov(opd, ptr(b), ptr(x), None, None, None, b.numel(), float(rtol), 0,
+                             int(bool(warm)))
+            need = (L.ttb_minres_work_doubles(C.byref(kd)) if method == "minres"
+                    else L.ttb_gmres_work_doubles(C.byref(kd), restart))
+            kd.work = ar.take(need).data_ptr()
+            descs.append(kd)
+        flags = ar.take_int(len(descs))
+        arr = (_lib.Krylov * len(descs))(*descs)
+        if method == "minres":
+            check(L.ttb_minres(arr, len(descs), flags.data_ptr(), stream()), "ttb_minres")
+        else:
+            check(L.ttb_gmres(arr, len(descs), restart, flags.data_ptr(), stream()), "ttb_gmres")
+
+
+def norm_many(items) -> None:
+    """items: (out, x, y or None)."""
+    if not items:
+        return
+    descs = [_lib.Norm(ptr(x), ptr(y), ptr(out), x.numel()) for out, x, y in items]
+    arr = (_lib.Norm * len(descs))(*descs)
+    check(lib().ttb_norm(arr, len(descs), stream()), "ttb_norm")
+
+
+def rank_residual_many(items) -> None:
+    """items: (contrib, b, exact, s, limit, damp, tol, rank_out)."""
+    if not items:
+        return
+    L = lib()
+    ar = arena()
+    with ar.scope():
+        descs = []
+        for contrib, b, exact, s, limit, damp, tol, rank_out in items:
+            n = b.numel()
+            work = ar.take(L.ttb_rank_work_doubles(n, limit))
+            descs.append(_lib.Rank(ptr(contrib), ptr(b), ptr(exact), ptr(s), ptr(rank_out),
+                                   ptr(work), n, limit, s.numel(), float(damp), float(tol)))
+        arr = (_lib.Rank * len(descs))(*descs)
+        check(L.ttb_rank_residual(arr, len(descs), stream()), "ttb_rank_residual")
+
+
+def rank_threshold_many(items) -> None:
+    """items: (s, mode, value, max_rank, rank_out)."""
+    if not items:
+        return
+    descs = [_lib.RankRule(ptr(s), ptr(out), s.numel(), int(mode), int(mr) if mr else 0,
+                           float(v)) for s, mode, v, mr, out in items]
+    arr = (_lib.RankRule * len(descs))(*descs)
+    check(lib().ttb_rank_threshold(arr, len(descs), stream()), "ttb_rank_threshold")
+
+
+def kron_many(items) -> List:
+    """items: (op, core); returns the Kronecker cores."""
+    if not items:
+        return []
+    outs, descs = [], []
+    for op, core in items:
+        ra, n, m, ra2 = op.shape
+        rx, m_, kk, rx2 = core.shape
+        out = empty(ra * rx, n, kk, ra2 * rx2)
+        outs.append(out)
+        descs.append(_lib.Kron(ptr(op), ptr(core), ptr(out), ra, ra2, n, m, rx, rx2, kk))
+    arr = (_lib.Kron * len(descs))(*descs)
+    check(lib().ttb_kron(arr, len(descs), stream()), "ttb_kron")
+    return outs
