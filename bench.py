@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--engine", default="auto", choices=["auto", "plain", "served"])
+    ap.add_argument("--engine", default="persistent", choices=["plain", "served", "persistent"])
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=0,
@@ -235,7 +235,14 @@ def fp64_peak_tflops(K, torch):
 
 
 class Engine:
-    """Solves a list of requests; returns per-request latencies (ms)."""
+    """Solves a list of requests; returns results and per-request latencies (ms).
+
+    ``plain``: one drop-in ``amen`` call after another; ``served``: the
+    lockstep batch engine; ``persistent``: one persistent launch in which
+    every request is a thread block running its whole solve.
+    """
+
+    RMAX = 64
 
     def __init__(self, kind: str):
         import torch
@@ -247,7 +254,13 @@ class Engine:
         self.torch = torch
 
     def upload(self, reqs):
+        """Inputs made resident on the device (not timed)."""
         tt = self.tt
+        if self.kind == "persistent":
+            from ttnumpy_b200.persistent import PersistentBatch, prepare
+
+            return PersistentBatch(prepare([(p.A, p.b, self.x0_host(p), solve_kwargs(p))
+                                            for p in reqs]), self.RMAX)
         out = []
         for p in reqs:
             A, b = tt.TensorTrain(p.A), tt.TensorTrain(p.b)
@@ -256,12 +269,36 @@ class Engine:
             out.append((A, b, x0, p))
         return out
 
-    def solve_all(self, dev_reqs, download: bool = False):
+    @staticmethod
+    def x0_host(p):
+        r = x0_cores(p)
+        if r is None:
+            return None
+        modes = [c.shape[1] for c in p.b]
+        ranks = [1] + [r] * (len(modes) - 1) + [1]
+        return [np.ones((ranks[i], modes[i], 1, ranks[i + 1])) for i in range(len(modes))]
+
+    def solve_all(self, handle, download: bool = False):
         torch = self.torch
+        if self.kind == "persistent":
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            handle.launch()
+            e.record()
+            res = handle.collect()
+            ms = s.elapsed_time(e)
+            for r in res:
+                if r.status != 0:
+                    raise RuntimeError(f"persistent solve failed with status {r.status}")
+            results = [(r.x, r.info) for r in res]
+            if download:
+                for x, _ in results:
+                    x.to_numpy()
+            return results, [ms] * len(results)
         lat = []
         results = []
         if self.kind == "plain":
-            for A, b, x0, p in dev_reqs:
+            for A, b, x0, p in handle:
                 s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s.record()
                 x, info = self.tt.amen(A, b, x0=x0, return_info=True, **solve_kwargs(p))
@@ -271,12 +308,10 @@ class Engine:
                 results.append((x, info))
                 lat.append((s, e))
             torch.cuda.synchronize()
-            lat = [s.elapsed_time(e) for s, e in lat]
-        else:
-            from ttnumpy_b200.serving import serve_batch
+            return results, [s.elapsed_time(e) for s, e in lat]
+        from ttnumpy_b200.serving import serve_batch
 
-            results, lat = serve_batch(dev_reqs, solve_kwargs, download=download)
-        return results, lat
+        return serve_batch(handle, solve_kwargs, download=download)
 
 
 def flush_l2(torch, buf):
@@ -333,13 +368,6 @@ def main():
 
     K.lib()
     engine_kind = args.engine
-    if engine_kind == "auto":
-        try:
-            import ttnumpy_b200.serving  # noqa: F401
-
-            engine_kind = "served"
-        except ImportError:
-            engine_kind = "plain"
     eng = Engine(engine_kind)
     dev_reqs = eng.upload(reqs)
     flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB > L2
@@ -353,8 +381,10 @@ def main():
         eng.solve_all(dev_reqs)
     barrier()
 
-    # which kernel class dominates: one profiled pass, all classes
     lib = K.lib()
+    if engine_kind == "persistent":
+        return persistent_main(args, eng, dev_reqs, reqs, flush, barrier, world, rank, local)
+    # which kernel class dominates: one profiled pass, all classes
     lib.ttb_profile_reset()
     lib.ttb_profile_enable((1 << 12) - 1)
     eng.solve_all(dev_reqs)
@@ -426,6 +456,73 @@ def main():
         torch.distributed.destroy_process_group()
 
 
+def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
+    """Timed region for the persistent engine: one launch per step."""
+    import torch
+
+    from ttnumpy_b200 import kernels as K
+
+    step_ms, ok, launches, lats, flops = [], 0, 0, [], 0.0
+    barrier()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            K.fill_(flush, 0.0)
+            torch.cuda.synchronize()
+            l0 = K.launch_count()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            batch.launch()
+            e.record()
+            torch.cuda.synchronize()
+            launches += K.launch_count() - l0 + 1
+            ms = s.elapsed_time(e)
+            step_ms.append(ms)
+            res = batch.collect()
+            ok += sum(1 for r in res if r.status == 0 and r.info.converged)
+            lats.extend([ms] * len(res))
+            flops += batch.gemm_flops()
+    barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ok * world / (total_ms * 1e-3)
+    e2e = e2e_run(eng, reqs, args, torch, flush)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    fp64 = fp64_peak_tflops(K, torch)
+    ach = flops / (sum(step_ms) * 1e-3) / 1e12
+    roof = {"kernel": "k_amen (ttb_amen_persistent)", "bound": "tensor", "unit": "TFLOP/s",
+            "achieved": ach, "peak": fp64, "peak_source": "measured FP64 FMA probe "
+            "(ttb_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
+            "frac": ach / fp64, "traffic": None,
+            "flops_counted": "2mnk of every dense product the blocks ran; QR/SVD/LU not counted",
+            "per_launch_us": 1e3 * sum(step_ms) / len(step_ms), "launches": len(step_ms)}
+    cpu = None
+    if world == 1:
+        n_sample = args.cpu_sample or min(len(reqs), max(2 * cpu_cores(), 8))
+        sample = cpu_sample(reqs, n_sample)
+        dt, res = cpu_run(sample, cpu_cores())
+        conv = sum(1 for r in res if str(r[1]) == "converged")
+        cpu = {"value": conv / dt, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+               "sample": f"{len(sample)} of the {len(reqs)} requests (same mix), one pass, "
+                         f"{cpu_cores()} single-threaded oracle workers"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config(args, reqs, "persistent"),
+            "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
+            "converged": f"{ok}/{len(reqs) * args.steps}", "roofline": roof,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 CLASS_NAMES = ["gemm", "copy", "kron", "norm", "local_matrix", "qr", "svd", "lu", "rank",
                "minres", "gmres", "round"]
 
@@ -464,38 +561,26 @@ def roofline(cls, rec, pk, fp64_tflops):
 
 def e2e_run(eng, reqs, args, torch, flush):
     """Same metric through the public API: each step uploads the requests
-    from pinned host memory and downloads the solutions."""
-    pinned = []
-    h2d = 0
-    for p in reqs:
-        A = [torch.from_numpy(np.ascontiguousarray(c)).pin_memory() for c in p.A]
-        b = [torch.from_numpy(np.ascontiguousarray(c)).pin_memory() for c in p.b]
-        h2d += sum(c.numel() * 8 for c in A + b)
-        pinned.append((A, b, p))
-    total, ok, d2h = 0.0, 0, 0
+    from host memory and downloads the solutions."""
+    from ttnumpy_b200 import kernels as K
+
+    total, ok, d2h, h2d = 0.0, 0, 0, 0
     steps = max(1, args.steps)
     for _ in range(steps):
-        K_fill = flush
-        from ttnumpy_b200 import kernels as K
-
-        K.fill_(K_fill, 0.0)
+        K.fill_(flush, 0.0)
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        tt = eng.tt
-        dev = []
-        for A, b, p in pinned:
-            At, bt = tt.TensorTrain(A), tt.TensorTrain(b)
-            r = x0_cores(p)
-            x0 = tt.ones(bt.physical_dims(), ranks=r).orthonormalize("right") if r else None
-            dev.append((At, bt, x0, p))
-        results, _ = eng.solve_all(dev, download=True)
+        handle = eng.upload(reqs)
+        results, _ = eng.solve_all(handle, download=False)
         host = [x.to_numpy() for x, _ in results]
         e.record()
         torch.cuda.synchronize()
         total += s.elapsed_time(e)
         ok += sum(1 for _, info in results if info.converged)
         d2h = sum(sum(c.nbytes for c in h) for h in host)
+        h2d = sum(sum(np.asarray(c).nbytes for c in p.A) + sum(np.asarray(c).nbytes for c in p.b)
+                  for p in reqs)
     return {"value": ok / (total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h}
 

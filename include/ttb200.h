@@ -377,6 +377,65 @@ typedef struct {
 long long ttb_round_work_doubles(int d, int max_mode, int max_bond);
 int ttb_round_batch(const ttb_round_t* problem, void* stream);
 
+
+/* ------------------------------------------------------------------------
+ * Whole AMEn solves on the device, one thread block per solve, all solves
+ * of the launch running concurrently: the amen() sweep
+ * (ttnumpy/solvers/amen.py:395-725) with the residual train fit
+ * (amen.py:162-224), environments, local solves (direct GEPP for at most
+ * direct_solve_size unknowns, else MINRES with the reference's true-residual
+ * restarts, common.py:729-809), residual-budget or threshold truncation
+ * (common.py:812-929), enrichment and the per-sweep relative residual
+ * (common.py:118-146), with every rank decision taken on the device.
+ *
+ * ``tasks`` is a DEVICE array of ``count`` task structs.  Per task, ``dims``
+ * (device ints) holds n[0..d-1], R[0..d], rb[0..d], x0 bonds[0..d] and
+ * z0 bonds[0..d]; A, b, x0 and z0 are packed core by core at the given
+ * offsets (z0: the random rank-kickrank start, drawn on the host as the
+ * reference does).  The solve keeps every core and environment in its
+ * ``slab`` (ttb_amen_slab_doubles() doubles); x bonds are capped at
+ * ``rmax`` (status -4 when a bond would exceed it).  Results: result[0]
+ * status (0 ok, -1 singular local system, -3 slab too small, -4 rank cap,
+ * -5 unsupported settings), result[1] sweeps run, result[2] stop reason
+ * (0 converged, 1 stagnated, 2 max sweeps), result[3] local solves,
+ * result[4] inexact local solves, result[5..5+d] x bonds;
+ * residuals[0..sweeps-1] and, from residuals[max_sweeps], the largest
+ * bond after each sweep; residuals[2 * max_sweeps] receives the FP64 FLOPs
+ * of the block's dense products (2 m n k each; factorisations not
+ * counted), residuals[2 * max_sweeps + 1] the operator applications and
+ * residuals[2 * max_sweeps + 2 .. + 8] SM cycles spent in environment
+ * updates, local solves, residual cores, truncation with enrichment, (unused),
+ * residual checks and set-up; x core k at slab + x_offsets[k].  local_rtol > 0
+ * selects MINRES for local systems above direct_solve_size unknowns (at
+ * most min(5 N, 2000) iterations per call, SciPy's cap being 5 N);
+ * local_rtol <= 0 refuses them (status -5).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* A;
+  const long long* A_off;
+  const double* b;
+  const long long* b_off;
+  const double* x0;
+  const long long* x0_off;
+  const double* z0;
+  const long long* z0_off;
+  const int* dims;
+  double* slab;
+  long long slab_doubles;
+  double* residuals;
+  int* result;
+  long long* x_offsets;
+  int d, kickrank, max_rank, max_sweeps, direct_solve_size, track_residual, residual_mode,
+      stagnation_on, x0_orth_center, b_orth_center;
+  double residual_tol, error_threshold, residual_damp, stagnation_factor, local_rtol,
+      truncation_tol;
+  int debug; /* 1: also apply the operator to every rank-one term in full and
+                record the worst relative gap in residuals[2*max_sweeps + 9] */
+} ttb_amen_task_t;
+long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int rmax,
+                                int direct_solve_size);
+int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,7 +40,8 @@ def test_struct_sizes_match_c():
              "ttb_qr_t": _lib.QR, "ttb_svd_t": _lib.SVD, "ttb_lu_t": _lib.LU,
              "ttb_copy_t": _lib.Copy, "ttb_kron_t": _lib.Kron, "ttb_norm_t": _lib.Norm,
              "ttb_rank_t": _lib.Rank, "ttb_rank_rule_t": _lib.RankRule,
-             "ttb_krylov_t": _lib.Krylov, "ttb_round_t": _lib.Round}
+             "ttb_krylov_t": _lib.Krylov, "ttb_round_t": _lib.Round,
+             "ttb_amen_task_t": _lib.AmenTask}
     src = '#include <stdio.h>\n#include "ttb200.h"\nint main(void){\n'
     for name in pairs:
         src += f'printf("%zu\\n", sizeof({name}));\n'

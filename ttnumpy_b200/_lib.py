@@ -100,6 +100,18 @@ class Round(C.Structure):
                 ("max_rank", I)]
 
 
+class AmenTask(C.Structure):
+    _fields_ = [("A", P), ("A_off", P), ("b", P), ("b_off", P), ("x0", P), ("x0_off", P),
+                ("z0", P), ("z0_off", P), ("dims", P), ("slab", P), ("slab_doubles", L),
+                ("residuals", P), ("result", P), ("x_offsets", P),
+                ("d", I), ("kickrank", I), ("max_rank", I), ("max_sweeps", I),
+                ("direct_solve_size", I), ("track_residual", I), ("residual_mode", I),
+                ("stagnation_on", I), ("x0_orth_center", I), ("b_orth_center", I),
+                ("residual_tol", D), ("error_threshold", D), ("residual_damp", D),
+                ("stagnation_factor", D), ("local_rtol", D), ("truncation_tol", D),
+                ("debug", I)]
+
+
 _SIGNATURES = {
     "ttb_version": ([], I),
     "ttb_launch_count": ([], L),
@@ -132,6 +144,8 @@ _SIGNATURES = {
     "ttb_gmres": ([C.POINTER(Krylov), I, I, P, P], I),
     "ttb_round_work_doubles": ([I, I, I], L),
     "ttb_round_batch": ([C.POINTER(Round), P], I),
+    "ttb_amen_slab_doubles": ([I, C.POINTER(C.c_int), I, I, I], L),
+    "ttb_amen_persistent": ([P, I, I, P], I),
 }
 
 _lib = None

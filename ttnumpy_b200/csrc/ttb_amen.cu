@@ -1,0 +1,1351 @@
+// Whole AMEn solves on the device: one thread block per solve.
+//
+// The block runs the reference sweep (ttnumpy/solvers/amen.py:395-725) end
+// to end with every rank decision taken on the device.  Cores and
+// environments live in the solve's slab (global memory) in fixed-capacity
+// slots sized for bonds up to rmax; per-step temporaries come from a stack
+// at the top of the slab.  Dense factorisations run in a shared-memory pool
+// when the matrix fits and fall back to the blocked global-memory variants
+// otherwise.  All control flow is uniform across the block: every decision
+// derives from block-wide reductions that all threads see identically.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+
+#include "ttb200.h"
+#include "ttb_device.cuh"
+
+namespace {
+
+using namespace ttb;
+
+constexpr int kD = 64;                 // most cores per train
+constexpr int kPoolBytes = 190 * 1024;  // dynamic shared-memory pool
+constexpr i64 kPoolD = kPoolBytes / 8;
+constexpr int kMaxRestarts = 4;        // common.py:230
+constexpr double kShrink = 1e-2;       // common.py:233
+constexpr int kMaxMinres = 2000;       // iteration cap of one MINRES call
+constexpr double kEps = 2.220446049250313e-16;
+
+enum { ST_OK = 0, ST_SINGULAR = -1, ST_SLAB = -3, ST_RANK = -4, ST_SETTINGS = -5 };
+enum { F_A = 0, F_B, F_ZB, F_ZAX, F_XZ };
+
+struct Sm {
+  int n[kD], R[kD + 1], rb[kD + 1], xb[kD + 1], zb[kD + 1];
+  i64 xo[kD], zo[kD];
+  i64 eo[2][5][kD];
+  double red[TTB_WARPS];
+  int redi[TTB_WARPS];
+  int ipiv[LNB];
+  int flag;
+  i64 stack0;
+  GemmSmem gsm;
+};
+
+struct Ctx {
+  const ttb_amen_task_t* T;
+  Sm* sm;
+  double* slab;
+  i64 cap, top;
+  double* pool;
+  int d, rmax, K;
+  int status;
+  double flops;  // FP64 FLOPs of the block's GEMMs (2 m n k each)
+  long long applies;      // one-site operator applications
+  double check;           // debug: worst relative gap of the factorised term products
+  long long cyc[8];       // SM cycles per phase (see PH_*)
+};
+
+// phases timed with clock64 for the per-solve breakdown
+enum { PH_ENV = 0, PH_SOLVE, PH_ZCORE, PH_TRUNC, PH_ENRICH, PH_RESID, PH_INIT, PH_N };
+
+__device__ double* take(Ctx& c, i64 n) {
+  n = (n + 31) & ~31LL;
+  if (c.top + n > c.cap) {
+    c.status = ST_SLAB;
+    return nullptr;
+  }
+  double* p = c.slab + c.top;
+  c.top += n;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+
+__device__ void vfill(double* x, i64 n, double v) {
+  for (i64 i = threadIdx.x; i < n; i += TTB_THREADS) x[i] = v;
+}
+
+__device__ void vcopy(double* y, const double* x, i64 n, double a = 1.0) {
+  for (i64 i = threadIdx.x; i < n; i += TTB_THREADS) y[i] = a * x[i];
+}
+
+__device__ double vdot(const double* x, const double* y, i64 n, double* red) {
+  double s = 0.0;
+  for (i64 i = threadIdx.x; i < n; i += TTB_THREADS) s = fma(x[i], y[i], s);
+  return block_sum(s, red);
+}
+
+__device__ double vnorm_diff(const double* x, const double* y, i64 n, double* red) {
+  double s = 0.0;
+  for (i64 i = threadIdx.x; i < n; i += TTB_THREADS) {
+    double v = y ? x[i] - y[i] : x[i];
+    s = fma(v, v, s);
+  }
+  return sqrt(block_sum(s, red));
+}
+
+__device__ void gemm(Ctx& c, CMat A, CMat B, Mat C, int M, int N, int K, double alpha,
+                     double beta) {
+  if (M <= 0 || N <= 0) return;
+  c.flops += 2.0 * M * N * (double)K;
+  cta_gemm(A, B, C, M, N, K, alpha, beta, c.sm->gsm);
+}
+
+// ---------------------------------------------------------------------------
+// environments (common.py:149-217), same GEMM chains as ttb_env_update
+// ---------------------------------------------------------------------------
+
+__device__ __noinline__ void env_step(Ctx& c, int side, const double* env, int t, int R, int f,
+                         const double* frame, int n, int f2, const double* op, int m, int R2,
+                         const double* target, int t2, double* out) {
+  const i64 mark = c.top;
+  if (op) {
+    if (side == 0) {
+      double* S1 = take(c, (i64)t * R * n * f2);
+      double* S2 = take(c, (i64)t * m * R2 * f2);
+      if (c.status) return;
+      gemm(c, CMat{env, f, 1}, CMat{frame, (i64)n * f2, 1}, Mat{S1, (i64)n * f2, 1}, t * R,
+           n * f2, f, 1.0, 0.0);
+      for (int tt = 0; tt < t; ++tt)
+        gemm(c, CMat{op, 1, (i64)m * R2}, CMat{S1 + (i64)tt * R * n * f2, f2, 1},
+             Mat{S2 + (i64)tt * m * R2 * f2, f2, 1}, m * R2, f2, R * n, 1.0, 0.0);
+      gemm(c, CMat{target, 1, t2}, CMat{S2, (i64)R2 * f2, 1}, Mat{out, (i64)R2 * f2, 1}, t2,
+           R2 * f2, t * m, 1.0, 0.0);
+    } else {
+      double* S1 = take(c, (i64)t2 * m * R * f);
+      double* S2 = take(c, (i64)t2 * R2 * n * f);
+      if (c.status) return;
+      gemm(c, CMat{target, t, 1}, CMat{env, (i64)R * f, 1}, Mat{S1, (i64)R * f, 1}, t2 * m,
+           R * f, t, 1.0, 0.0);
+      for (int tt = 0; tt < t2; ++tt)
+        gemm(c, CMat{op, (i64)m * R, 1}, CMat{S1 + (i64)tt * m * R * f, f, 1},
+             Mat{S2 + (i64)tt * R2 * n * f, f, 1}, R2 * n, f, m * R, 1.0, 0.0);
+      gemm(c, CMat{S2, (i64)n * f, 1}, CMat{frame, 1, (i64)n * f}, Mat{out, f2, 1}, t2 * R2, f2,
+           n * f, 1.0, 0.0);
+    }
+  } else {
+    if (side == 0) {
+      double* S1 = take(c, (i64)t * n * f2);
+      if (c.status) return;
+      gemm(c, CMat{env, f, 1}, CMat{frame, (i64)n * f2, 1}, Mat{S1, (i64)n * f2, 1}, t, n * f2,
+           f, 1.0, 0.0);
+      gemm(c, CMat{target, 1, t2}, CMat{S1, f2, 1}, Mat{out, f2, 1}, t2, f2, t * n, 1.0, 0.0);
+    } else {
+      double* S1 = take(c, (i64)t2 * n * f);
+      if (c.status) return;
+      gemm(c, CMat{target, t, 1}, CMat{env, f, 1}, Mat{S1, f, 1}, t2 * n, f, t, 1.0, 0.0);
+      gemm(c, CMat{S1, (i64)n * f, 1}, CMat{frame, 1, (i64)n * f}, Mat{out, f2, 1}, t2, f2,
+           n * f, 1.0, 0.0);
+    }
+  }
+  c.top = mark;
+}
+
+__device__ double* xcore(Ctx& c, int k) { return c.slab + c.sm->xo[k]; }
+__device__ double* zcore(Ctx& c, int k) { return c.slab + c.sm->zo[k]; }
+__device__ const double* acore(Ctx& c, int k) { return c.T->A + c.T->A_off[k]; }
+__device__ const double* bcore(Ctx& c, int k) { return c.T->b + c.T->b_off[k]; }
+__device__ double* envp(Ctx& c, int side, int fam, int k) { return c.slab + c.sm->eo[side][fam][k]; }
+
+// Environment of family ``fam`` at site k from its neighbour (left: from
+// k - 1, right: from k + 1); the boundary ones are ones.
+__device__ __noinline__ void build_env(Ctx& c, int side, int fam, int k) {
+  Sm* s = c.sm;
+  const int d = c.d;
+  double* out = envp(c, side, fam, k);
+  if ((side == 0 && k == 0) || (side == 1 && k == d - 1)) {
+    if (threadIdx.x == 0) out[0] = 1.0;
+    __syncthreads();
+    return;
+  }
+  const int src = side == 0 ? k - 1 : k + 1;     // core contracted
+  const int pin = side == 0 ? k - 1 : k + 2;     // bond of the previous env
+  const int pout = side == 0 ? k : k + 1;        // bond of the new env
+  const int psrc = side == 0 ? k - 1 : k + 1;    // previous env index
+  const double* prev = envp(c, side, fam, psrc);
+  const int n = s->n[src];
+  const double* xc = xcore(c, src);
+  const double* zc = zcore(c, src);
+  const double* bc = bcore(c, src);
+  const double* ac = acore(c, src);
+  switch (fam) {
+    case F_A:
+      env_step(c, side, prev, s->xb[pin], s->R[pin], s->xb[pin], xc, n, s->xb[pout], ac, n,
+               s->R[pout], xc, s->xb[pout], out);
+      break;
+    case F_B:
+      env_step(c, side, prev, s->rb[pin], 1, s->xb[pin], xc, n, s->xb[pout], nullptr, n, 1, bc,
+               s->rb[pout], out);
+      break;
+    case F_ZB:
+      env_step(c, side, prev, s->rb[pin], 1, s->zb[pin], zc, n, s->zb[pout], nullptr, n, 1, bc,
+               s->rb[pout], out);
+      break;
+    case F_ZAX:
+      env_step(c, side, prev, s->xb[pin], s->R[pin], s->zb[pin], zc, n, s->zb[pout], ac, n,
+               s->R[pout], xc, s->xb[pout], out);
+      break;
+    default:
+      env_step(c, side, prev, s->zb[pin], 1, s->xb[pin], xc, n, s->xb[pout], nullptr, n, 1, zc,
+               s->zb[pout], out);
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// one-site local operator and projections
+// ---------------------------------------------------------------------------
+
+struct LocalOp {
+  const double* left;
+  const double* op;
+  const double* right;
+  int lt, lf, R, R2, n, m, rt, rf;
+};
+
+__device__ LocalOp local_A(Ctx& c, int k) {
+  Sm* s = c.sm;
+  LocalOp L;
+  L.left = envp(c, 0, F_A, k);
+  L.right = envp(c, 1, F_A, k);
+  L.op = acore(c, k);
+  L.lt = L.lf = s->xb[k];
+  L.rt = L.rf = s->xb[k + 1];
+  L.R = s->R[k];
+  L.R2 = s->R[k + 1];
+  L.n = L.m = s->n[k];
+  return L;
+}
+
+// y = alpha * B x + beta * y for ``cols`` vectors (ttb_local_apply's chain)
+__device__ __noinline__ void apply(Ctx& c, const LocalOp& L, const double* x, double* y, int cols,
+                      double alpha, double beta) {
+  const i64 mark = c.top;
+  c.applies += cols;
+  double* T1 = take(c, (i64)cols * L.lt * L.m * L.R2 * L.rf);
+  double* T2 = take(c, (i64)cols * L.lt * L.R * L.n * L.rf);
+  if (c.status) return;
+  gemm(c, CMat{x, L.rt, 1}, CMat{L.right, (i64)L.R2 * L.rf, 1}, Mat{T1, (i64)L.R2 * L.rf, 1},
+       cols * L.lt * L.m, L.R2 * L.rf, L.rt, 1.0, 0.0);
+  for (int ci = 0; ci < cols * L.lt; ++ci)
+    gemm(c, CMat{L.op, (i64)L.m * L.R2, 1}, CMat{T1 + (i64)ci * L.m * L.R2 * L.rf, L.rf, 1},
+         Mat{T2 + (i64)ci * L.R * L.n * L.rf, L.rf, 1}, L.R * L.n, L.rf, L.m * L.R2, 1.0, 0.0);
+  for (int cc = 0; cc < cols; ++cc)
+    gemm(c, CMat{L.left, 1, L.lf}, CMat{T2 + (i64)cc * L.lt * L.R * L.n * L.rf, (i64)L.n * L.rf, 1},
+         Mat{y + (i64)cc * L.lf * L.n * L.rf, (i64)L.n * L.rf, 1}, L.lf, L.n * L.rf, L.lt * L.R,
+         alpha, beta);
+  c.top = mark;
+}
+
+// out (i, n, l) = alpha * Lb^T core Rb + beta * out (local_rhs_one_site)
+__device__ __noinline__ void project(Ctx& c, const double* left, int a, int i, const double* core, int n,
+                        int cc, const double* right, int l, double* out, double alpha,
+                        double beta) {
+  const i64 mark = c.top;
+  double* W = take(c, (i64)a * n * l);
+  if (c.status) return;
+  gemm(c, CMat{core, cc, 1}, CMat{right, l, 1}, Mat{W, l, 1}, a * n, l, cc, 1.0, 0.0);
+  gemm(c, CMat{left, 1, i}, CMat{W, (i64)n * l, 1}, Mat{out, (i64)n * l, 1}, i, n * l, a, alpha,
+       beta);
+  c.top = mark;
+}
+
+// ---------------------------------------------------------------------------
+// factorisations with the shared pool or the blocked global variants
+// ---------------------------------------------------------------------------
+
+// Economic QR of the m x k view A: Q (m x p) and R (p x k) strided outputs.
+__device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
+  const int p = min(m, k);
+  if ((i64)m * k + p <= kPoolD) {
+    cta_qr(A, m, k, c.pool, c.pool + (i64)m * k, Q, R, c.sm->red);
+    return;
+  }
+  const i64 mark = c.top;
+  double* W = take(c, (i64)m * k + p);
+  if (c.status) return;
+  double* Y = c.pool;
+  double* G = Y + (i64)LNB * YCH;
+  double* Tm = G + LNB * LNB;
+  cta_qr_blocked(A, m, k, W, W + (i64)m * k, Q, R, Y, G, Tm, c.sm->red, c.sm->gsm);
+  c.top = mark;
+}
+
+// Thin SVD of the m x k view A into U (m x p), S (p), Vh (p x k).
+__device__ __noinline__ void svd(Ctx& c, CMat A, int m, int k, Mat U, double* S, Mat Vh) {
+  const bool tall = m >= k;
+  const int M = tall ? m : k, K = tall ? k : m;
+  CMat At = tall ? A : CMat{A.p, A.cs, A.rs};
+  Mat Ut = tall ? U : Mat{Vh.p, Vh.cs, Vh.rs};
+  Mat Vt = tall ? Vh : Mat{U.p, U.cs, U.rs};
+  const i64 need = (i64)M * K + 2 * (i64)K * K + 3 * (i64)K + 2;
+  const i64 mark = c.top;
+  double* base;
+  const bool in_pool = need <= kPoolD;
+  if (in_pool) {
+    base = c.pool;
+  } else {
+    base = take(c, need);
+    if (c.status) return;
+  }
+  double* W = base;
+  double* tau = W + (i64)M * K;
+  double* Bsq = tau + K;
+  double* V = Bsq + (i64)K * K;
+  double* sv = V + (i64)K * K;
+  int* order = reinterpret_cast<int*>(sv + K);
+  int* flag = reinterpret_cast<int*>(sv + 2 * K);
+  if (in_pool) {
+    cta_svd_tall(At, M, K, W, tau, Bsq, V, sv, order, flag, Ut, S, Vt, c.sm->red);
+  } else {
+    double* Y = c.pool;
+    double* G = Y + (i64)LNB * YCH;
+    double* Tm = G + LNB * LNB;
+    cta_svd_tall_blocked(At, M, K, W, tau, Bsq, V, sv, order, flag, Ut, S, Vt, Y, G, Tm,
+                         c.sm->red, c.sm->gsm);
+  }
+  c.top = mark;
+}
+
+// ---------------------------------------------------------------------------
+// local solves
+// ---------------------------------------------------------------------------
+
+// Explicit local matrix (column major, n x n) and GEPP solve; u <- solution.
+__device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double* b, double* u) {
+  const i64 N = (i64)L.lf * L.n * L.rf;
+  const i64 mark = c.top;
+  Sm* s = c.sm;
+  double* W;
+  const bool small = N * N + N <= kPoolD;
+  if (small) {
+    W = c.pool;
+  } else {
+    if (N * LNB > kPoolD) {
+      c.status = ST_SETTINGS;
+      return;
+    }
+    W = take(c, N * N);
+    if (c.status) return;
+  }
+  for (i64 e = threadIdx.x; e < N * N; e += TTB_THREADS) {
+    i64 row = e % N, col = e / N;
+    int nf = (int)(row % L.rf), kr = (int)((row / L.rf) % L.n), j = (int)(row / ((i64)L.rf * L.n));
+    int mt = (int)(col % L.rt), l = (int)((col / L.rt) % L.m), i = (int)(col / ((i64)L.rt * L.m));
+    double acc = 0.0;
+    for (int a = 0; a < L.R; ++a) {
+      const double la = L.left[((i64)i * L.R + a) * L.lf + j];
+      if (la == 0.0) continue;
+      const double* op = L.op + (((i64)a * L.n + kr) * L.m + l) * L.R2;
+      double t = 0.0;
+      for (int bb = 0; bb < L.R2; ++bb) t = fma(op[bb], L.right[((i64)mt * L.R2 + bb) * L.rf + nf], t);
+      acc = fma(la, t, acc);
+    }
+    W[e] = acc;
+  }
+  vcopy(u, b, N);
+  __syncthreads();
+  int info;
+  if (small) {
+    // b goes to the pool too so the whole solve stays on chip
+    double* bb = c.pool + N * N;
+    vcopy(bb, u, N);
+    __syncthreads();
+    info = cta_gepp_solve(W, N, bb, (int)N, s->red, s->redi);
+    __syncthreads();
+    if (info == 0) vcopy(u, bb, N);
+  } else {
+    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, s->gsm);
+  }
+  __syncthreads();
+  if (info != 0) c.status = ST_SINGULAR;
+  c.top = mark;
+}
+
+// MINRES, SciPy 1.18.1's algorithm and stopping rules (Paige & Saunders);
+// x holds the initial guess (warm) on entry and the iterate on exit.
+__device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, double* x, i64 N, double rtol,
+                       int maxit, bool warm) {
+  double* red = c.sm->red;
+  const i64 mark = c.top;
+  double* buf = take(c, 7 * N);
+  if (c.status) return;
+  double* r1 = buf;
+  double* r2 = buf + N;
+  double* y = buf + 2 * N;
+  double* v = buf + 3 * N;
+  double* w = buf + 4 * N;
+  double* w1 = buf + 5 * N;
+  double* w2 = buf + 6 * N;
+  if (warm) {
+    apply(c, L, x, y, 1, 1.0, 0.0);
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) r1[i] = b[i] - y[i];
+  } else {
+    vfill(x, N, 0.0);
+    vcopy(r1, b, N);
+  }
+  __syncthreads();
+  const double beta1sq = vdot(r1, r1, N, red);
+  const double bnorm = sqrt(vdot(b, b, N, red));
+  if (beta1sq == 0.0 || bnorm == 0.0) {
+    if (bnorm == 0.0) vcopy(x, b, N);
+    __syncthreads();
+    c.top = mark;
+    return;
+  }
+  const double beta1 = sqrt(beta1sq);
+  double oldb = 0.0, beta = beta1, dbar = 0.0, epsln = 0.0, phibar = beta1, rhs1 = beta1,
+         rhs2 = 0.0, tnorm2 = 0.0, gmax = 0.0, gmin = DBL_MAX, cs = -1.0, sn = 0.0;
+  vfill(w, N, 0.0);
+  vfill(w2, N, 0.0);
+  vcopy(r2, r1, N);
+  vcopy(y, r1, N);
+  __syncthreads();
+  int istop = 0;
+  for (int itn = 1; itn <= maxit; ++itn) {
+    const double s = 1.0 / beta;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) v[i] = s * y[i];
+    __syncthreads();
+    apply(c, L, v, y, 1, 1.0, 0.0);
+    if (c.status) return;
+    if (itn >= 2) {
+      const double f = beta / oldb;
+      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) y[i] -= f * r1[i];
+      __syncthreads();
+    }
+    const double alfa = vdot(v, y, N, red);
+    const double g = alfa / beta;
+    double part = 0.0;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+      double yi = y[i] - g * r2[i];
+      r1[i] = r2[i];
+      r2[i] = yi;
+      y[i] = yi;
+      part = fma(yi, yi, part);
+    }
+    oldb = beta;
+    beta = sqrt(block_sum(part, red));
+    tnorm2 += alfa * alfa + oldb * oldb + beta * beta;
+    if (itn == 1 && beta / beta1 <= 10.0 * kEps) istop = -1;
+    const double oldeps = epsln;
+    const double delta = cs * dbar + sn * alfa;
+    const double gbar = sn * dbar - cs * alfa;
+    epsln = sn * beta;
+    dbar = -cs * beta;
+    const double root = hypot(gbar, dbar);
+    double gamma = fmax(hypot(gbar, beta), kEps);
+    cs = gbar / gamma;
+    sn = beta / gamma;
+    const double phi = cs * phibar;
+    phibar = sn * phibar;
+    const double denom = 1.0 / gamma;
+    double xs = 0.0;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+      double a1 = w2[i], a2 = w[i];
+      double wn = (v[i] - oldeps * a1 - delta * a2) * denom;
+      w1[i] = a1;
+      w2[i] = a2;
+      w[i] = wn;
+      double xi = x[i] + phi * wn;
+      x[i] = xi;
+      xs = fma(xi, xi, xs);
+    }
+    gmax = fmax(gmax, gamma);
+    gmin = fmin(gmin, gamma);
+    const double z = rhs1 / gamma;
+    rhs1 = rhs2 - delta * z;
+    rhs2 = -epsln * z;
+    const double Anorm = sqrt(tnorm2);
+    const double ynorm = sqrt(block_sum(xs, red));
+    const double epsx = Anorm * ynorm * kEps;
+    const double rnorm = phibar;
+    const double test1 = (ynorm == 0.0 || Anorm == 0.0) ? INFINITY : rnorm / (Anorm * ynorm);
+    const double test2 = (Anorm == 0.0) ? INFINITY : root / Anorm;
+    const double Acond = gmax / gmin;
+    if (istop == 0) {
+      if (1.0 + test2 <= 1.0) istop = 2;
+      if (1.0 + test1 <= 1.0) istop = 1;
+      if (itn >= maxit) istop = 6;
+      if (Acond >= 0.1 / kEps) istop = 4;
+      if (epsx >= beta1) istop = 3;
+      if (test2 <= rtol) istop = 2;
+      if (test1 <= rtol) istop = 1;
+    }
+    if (istop != 0) break;
+  }
+  __syncthreads();
+  c.top = mark;
+}
+
+// _solve_local_system (common.py:729-809): u <- solution of B u = b.
+__device__ __noinline__ void solve_local(Ctx& c, int k, const double* b_loc, double* u, int* nsolves,
+                            int* ninexact) {
+  const ttb_amen_task_t* T = c.T;
+  LocalOp L = local_A(c, k);
+  const i64 N = (i64)L.lf * L.n * L.rf;
+  if (N <= T->direct_solve_size) {
+    direct_solve(c, L, b_loc, u);
+    return;
+  }
+  if (T->local_rtol <= 0.0) {  // iterative solves need MINRES settings
+    c.status = ST_SETTINGS;
+    return;
+  }
+  vcopy(u, xcore(c, k), N);  // warm start: the current centre core
+  __syncthreads();
+  const i64 mark = c.top;
+  double* tmp = take(c, N);
+  if (c.status) return;
+  const double bn = vnorm_diff(b_loc, nullptr, N, c.sm->red);
+  double rtol = T->local_rtol;
+  // SciPy's default cap is 5 N iterations; a block solving alone on one SM
+  // is bounded tighter so that no launch runs unbounded on a shared GPU
+  const int maxit = (int)min(5 * N, (i64)kMaxMinres);
+  for (int attempt = 0; attempt < kMaxRestarts; ++attempt) {
+    minres(c, L, b_loc, u, N, rtol, maxit, true);
+    if (c.status) return;
+    apply(c, L, u, tmp, 1, 1.0, 0.0);
+    const double rn = vnorm_diff(tmp, b_loc, N, c.sm->red);
+    if (rn <= T->local_rtol * bn) {
+      *nsolves += 1;
+      c.top = mark;
+      return;
+    }
+    rtol = fmax(rtol * kShrink, 1e-15);
+  }
+  *nsolves += 1;
+  *ninexact += 1;
+  c.top = mark;
+}
+
+// ---------------------------------------------------------------------------
+// truncation rank (common.py:812-929)
+// ---------------------------------------------------------------------------
+
+// The operator applied to the r-th rank-one term of the solved core,
+// C = B (s_r U[:, r] (x) Vh[r, :]), using the factorisation of B over the
+// operator bond: for a forward (right-bond) split the term is u (lt, m) (x)
+// v (rt) and C[j, k, q] = sum_{a,b} (L_a^T A_ab u)[j, k] (R_b v)[q]; for a
+// backward split the term is u (lt) (x) v (m, rt) and
+// C[j, k, q] = sum_{a,b} (L_a^T u)[j] (A_ab V R_b)[k, q].  Same values as a
+// full application of B to the term (up to rounding) at O(R R2 n^2 r)
+// instead of O(n R r^3 + n^2 R^2 r^2) work.
+__device__ __noinline__ void rank1_apply(Ctx& c, const LocalOp& L, bool forward, const double* U,
+                                         const double* S, const double* Vh, int p, int r,
+                                         double* out) {
+  const int lt = L.lt, lf = L.lf, R = L.R, R2 = L.R2, n = L.n, m = L.m, rt = L.rt, rf = L.rf;
+  const double sr = S[r];
+  const i64 mark = c.top;
+  if (forward) {
+    // u_r[i, l] = s_r U[(i, l), r]; v_r[p'] = Vh[r, p']
+    double* P = take(c, (i64)R * lf * m);
+    double* Y = take(c, (i64)lf * n * R2);
+    double* W = take(c, (i64)R2 * rf);
+    if (c.status) return;
+    for (int a = 0; a < R; ++a)
+      gemm(c, CMat{L.left + (i64)a * lf, 1, (i64)R * lf}, CMat{U + r, (i64)m * p, p},
+           Mat{P + (i64)a * lf * m, m, 1}, lf, m, lt, sr, 0.0);
+    for (int a = 0; a < R; ++a)
+      for (int b = 0; b < R2; ++b)
+        gemm(c, CMat{P + (i64)a * lf * m, m, 1},
+             CMat{L.op + (i64)a * n * m * R2 + b, R2, (i64)m * R2},
+             Mat{Y + b, (i64)n * R2, R2}, lf, n, m, 1.0, a == 0 ? 0.0 : 1.0);
+    gemm(c, CMat{Vh + (i64)r * rt, 0, 1}, CMat{L.right, (i64)R2 * rf, 1}, Mat{W, 0, 1}, 1,
+         R2 * rf, rt, 1.0, 0.0);
+    gemm(c, CMat{Y, R2, 1}, CMat{W, rf, 1}, Mat{out, rf, 1}, lf * n, rf, R2, 1.0, 0.0);
+  } else {
+    // u_r[i] = s_r U[i, r]; v_r[l, p'] = Vh[r, (l, p')]
+    double* yv = take(c, (i64)R * lf);
+    double* Q = take(c, (i64)m * R2 * rf);
+    double* Z = take(c, (i64)R * n * rf);
+    if (c.status) return;
+    gemm(c, CMat{U + r, 0, p}, CMat{L.left, (i64)R * lf, 1}, Mat{yv, 0, 1}, 1, R * lf, lt, sr,
+         0.0);
+    gemm(c, CMat{Vh + (i64)r * m * rt, rt, 1}, CMat{L.right, (i64)R2 * rf, 1},
+         Mat{Q, (i64)R2 * rf, 1}, m, R2 * rf, rt, 1.0, 0.0);
+    for (int a = 0; a < R; ++a)
+      for (int b = 0; b < R2; ++b)
+        gemm(c, CMat{L.op + (i64)a * n * m * R2 + b, (i64)m * R2, R2},
+             CMat{Q + (i64)b * rf, (i64)R2 * rf, 1}, Mat{Z + (i64)a * n * rf, rf, 1}, n, rf, m,
+             1.0, b == 0 ? 0.0 : 1.0);
+    gemm(c, CMat{yv, 1, lf}, CMat{Z, (i64)n * rf, 1}, Mat{out, (i64)n * rf, 1}, lf, n * rf, R,
+         1.0, 0.0);
+  }
+  c.top = mark;
+}
+
+// U (M x p, col stride p... row major M x p), S (p), Vh (p x Kc row major):
+// the solved core u = U diag(S) Vh as a vector of length M * Kc.
+__device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const double* b_loc, const double* U,
+                           const double* S, const double* Vh, int M, int Kc, int p) {
+  const ttb_amen_task_t* T = c.T;
+  double* red = c.sm->red;
+  if (!T->residual_mode) {
+    if (p <= 0 || S[0] == 0.0) return 1;
+    int cnt = 0;
+    for (int i = 0; i < p; ++i) cnt += (S[i] / S[0] > T->error_threshold);
+    int r = max(cnt, 1);
+    if (T->max_rank > 0 && r > T->max_rank) r = T->max_rank;
+    return r;
+  }
+  if (S[0] == 0.0) return 1;
+  int limit = p;
+  if (T->max_rank > 0) limit = min(limit, T->max_rank);
+  LocalOp L = local_A(c, k);
+  const i64 N = (i64)M * Kc;
+  const i64 mark = c.top;
+  double* tmp = take(c, N);
+  double* part = take(c, N);
+  double* term = take(c, N);
+  if (c.status) return 1;
+  apply(c, L, u, tmp, 1, 1.0, 0.0);
+  const double exact = vnorm_diff(tmp, b_loc, N, red);
+  const double bn = vnorm_diff(b_loc, nullptr, N, red);
+  const double thr = fmax(T->residual_damp * exact, 0.5 * T->truncation_tol * bn);
+  for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) part[i] = -b_loc[i];
+  __syncthreads();
+  int rank = limit;
+  const bool forward = (M == L.lt * L.m);
+  for (int r = 0; r < limit; ++r) {
+    rank1_apply(c, L, forward, U, S, Vh, p, r, tmp);
+    if (c.status) return 1;
+    if (T->debug) {
+      // the full application of B to the term, for the self-check
+      const double sr = S[r];
+      for (i64 e = threadIdx.x; e < N; e += TTB_THREADS) {
+        i64 i = e / Kc, j = e % Kc;
+        term[e] = (U[i * p + r] * sr) * Vh[(i64)r * Kc + j];
+      }
+      __syncthreads();
+      double* full = take(c, N);
+      if (c.status) return 1;
+      apply(c, L, term, full, 1, 1.0, 0.0);
+      double dmax = 0.0, fmax_ = 0.0;
+      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+        dmax = fmax(dmax, fabs(full[i] - tmp[i]));
+        fmax_ = fmax(fmax_, fabs(full[i]));
+      }
+      // block max via the sum slots: one warp value per warp, then serial
+      for (int o = 16; o > 0; o >>= 1) {
+        dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
+        fmax_ = fmax(fmax_, __shfl_down_sync(0xffffffffu, fmax_, o));
+      }
+      __syncthreads();
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = fmax_ > 0.0 ? dmax / fmax_ : dmax;
+      __syncthreads();
+      double worst = 0.0;
+      for (int w = 0; w < TTB_WARPS; ++w) worst = fmax(worst, red[w]);
+      c.check = fmax(c.check, worst);
+      __syncthreads();
+      c.top -= ((N + 31) & ~31LL);
+    }
+    double s = 0.0;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+      double v = part[i] + tmp[i];
+      part[i] = v;
+      s = fma(v, v, s);
+    }
+    if (sqrt(block_sum(s, red)) <= thr) {
+      rank = r + 1;
+      break;
+    }
+  }
+  c.top = mark;
+  return rank;
+}
+
+// ---------------------------------------------------------------------------
+// centre shifts and enrichment
+// ---------------------------------------------------------------------------
+
+// z core k <- Q of core (zl, n, zr); z core k+1 <- R z core k+1 (in place
+// through a temporary), zb[k+1] = p.
+__device__ __noinline__ void z_shift_right(Ctx& c, int k, const double* core, int zl, int n, int zr) {
+  Sm* s = c.sm;
+  const int p = min(zl * n, zr);
+  const i64 mark = c.top;
+  double* R = take(c, (i64)p * zr);
+  const int n2 = s->n[k + 1], zr2 = s->zb[k + 2];
+  double* nxt = take(c, (i64)p * n2 * zr2);
+  if (c.status) return;
+  qr(c, CMat{core, zr, 1}, zl * n, zr, Mat{zcore(c, k), p, 1}, Mat{R, zr, 1});
+  gemm(c, CMat{R, zr, 1}, CMat{zcore(c, k + 1), (i64)n2 * zr2, 1}, Mat{nxt, (i64)n2 * zr2, 1}, p,
+       n2 * zr2, zr, 1.0, 0.0);
+  vcopy(zcore(c, k + 1), nxt, (i64)p * n2 * zr2);
+  __syncthreads();
+  if (threadIdx.x == 0) s->zb[k + 1] = p;
+  __syncthreads();
+  c.top = mark;
+}
+
+__device__ __noinline__ void z_shift_left(Ctx& c, int k, const double* core, int zl, int n, int zr) {
+  Sm* s = c.sm;
+  const int p = min(zl, n * zr);
+  const i64 mark = c.top;
+  double* R = take(c, (i64)p * zl);
+  const int zpp = s->zb[k - 1], n0 = s->n[k - 1];
+  double* prv = take(c, (i64)zpp * n0 * p);
+  if (c.status) return;
+  // Q^T of core^T goes straight into the slot as (p, n, zr)
+  qr(c, CMat{core, 1, (i64)n * zr}, n * zr, zl, Mat{zcore(c, k), 1, (i64)n * zr},
+     Mat{R, zl, 1});
+  gemm(c, CMat{zcore(c, k - 1), zl, 1}, CMat{R, 1, zl}, Mat{prv, p, 1}, zpp * n0, p, zl, 1.0, 0.0);
+  vcopy(zcore(c, k - 1), prv, (i64)zpp * n0 * p);
+  __syncthreads();
+  if (threadIdx.x == 0) s->zb[k] = p;
+  __syncthreads();
+  c.top = mark;
+}
+
+// generic right-orthonormalisation of the x or z train from ``start`` to 1
+__device__ __noinline__ void orth_right(Ctx& c, bool isx, int start) {
+  Sm* s = c.sm;
+  int* bonds = isx ? s->xb : s->zb;
+  for (int i = start; i >= 1; --i) {
+    const int rl = bonds[i], n = s->n[i], rr = bonds[i + 1];
+    const int p = min(rl, n * rr);
+    const i64 mark = c.top;
+    double* core = take(c, (i64)rl * n * rr);
+    double* R = take(c, (i64)p * rl);
+    const int rpp = bonds[i - 1], n0 = s->n[i - 1];
+    double* prv = take(c, (i64)rpp * n0 * p);
+    if (c.status) return;
+    double* slot = isx ? xcore(c, i) : zcore(c, i);
+    double* pslot = isx ? xcore(c, i - 1) : zcore(c, i - 1);
+    vcopy(core, slot, (i64)rl * n * rr);
+    __syncthreads();
+    qr(c, CMat{core, 1, (i64)n * rr}, n * rr, rl, Mat{slot, 1, (i64)n * rr}, Mat{R, rl, 1});
+    gemm(c, CMat{pslot, rl, 1}, CMat{R, 1, rl}, Mat{prv, p, 1}, rpp * n0, p, rl, 1.0, 0.0);
+    if (isx && p > c.rmax) {
+      c.status = ST_RANK;
+      return;
+    }
+    vcopy(pslot, prv, (i64)rpp * n0 * p);
+    __syncthreads();
+    if (threadIdx.x == 0) bonds[i] = p;
+    __syncthreads();
+    c.top = mark;
+  }
+}
+
+__device__ __noinline__ void orth_left(Ctx& c, int end) {
+  Sm* s = c.sm;
+  for (int i = 0; i < end; ++i) {
+    const int rl = s->xb[i], n = s->n[i], rr = s->xb[i + 1];
+    const int p = min(rl * n, rr);
+    const i64 mark = c.top;
+    double* core = take(c, (i64)rl * n * rr);
+    double* R = take(c, (i64)p * rr);
+    const int n2 = s->n[i + 1], r2 = s->xb[i + 2];
+    double* nxt = take(c, (i64)p * n2 * r2);
+    if (c.status) return;
+    vcopy(core, xcore(c, i), (i64)rl * n * rr);
+    __syncthreads();
+    qr(c, CMat{core, rr, 1}, rl * n, rr, Mat{xcore(c, i), p, 1}, Mat{R, rr, 1});
+    gemm(c, CMat{R, rr, 1}, CMat{xcore(c, i + 1), (i64)n2 * r2, 1}, Mat{nxt, (i64)n2 * r2, 1}, p,
+         n2 * r2, rr, 1.0, 0.0);
+    vcopy(xcore(c, i + 1), nxt, (i64)p * n2 * r2);
+    __syncthreads();
+    if (threadIdx.x == 0) s->xb[i + 1] = p;
+    __syncthreads();
+    c.top = mark;
+  }
+}
+
+// residual core z (amen.py:109-159) of the solved core u at site k
+__device__ __noinline__ void residual_core(Ctx& c, int k, const double* u, double* out) {
+  Sm* s = c.sm;
+  const int zl = s->zb[k], zr = s->zb[k + 1], n = s->n[k];
+  project(c, envp(c, 0, F_ZB, k), s->rb[k], zl, bcore(c, k), n, s->rb[k + 1],
+          envp(c, 1, F_ZB, k), zr, out, 1.0, 0.0);
+  LocalOp L;
+  L.left = envp(c, 0, F_ZAX, k);
+  L.right = envp(c, 1, F_ZAX, k);
+  L.op = acore(c, k);
+  L.lt = s->xb[k];
+  L.lf = zl;
+  L.rt = s->xb[k + 1];
+  L.rf = zr;
+  L.R = s->R[k];
+  L.R2 = s->R[k + 1];
+  L.n = L.m = n;
+  apply(c, L, u, out, 1, -1.0, 1.0);
+}
+
+// forward step after the solve: truncate, enrich, shift x and z
+__device__ __noinline__ void forward_update(Ctx& c, int k, const double* u, const double* b_loc,
+                               const double* znew) {
+  Sm* s = c.sm;
+  const int rl = s->xb[k], n = s->n[k], rr = s->xb[k + 1];
+  const int zl = s->zb[k], zr = s->zb[k + 1];
+  const int M = rl * n, p = min(M, rr);
+  const i64 mark = c.top;
+  double* U = take(c, (i64)M * p);
+  double* S = take(c, p);
+  double* Vh = take(c, (i64)p * rr);
+  if (c.status) return;
+  svd(c, CMat{u, rr, 1}, M, rr, Mat{U, p, 1}, S, Mat{Vh, rr, 1});
+  __syncthreads();
+  const int rank = choose_rank(c, k, u, b_loc, U, S, Vh, M, rr, p);
+  if (c.status) return;
+  const int cols = rank + zr;
+  const int n2 = s->n[k + 1], r2 = s->xb[k + 2];
+  double* enr = take(c, (i64)M * cols);
+  double* padded = take(c, (i64)cols * n2 * r2);
+  if (c.status) return;
+  // enriched = [U[:, :rank] | block], block (rl, n, zr) = lxz^T z_new
+  double* block = take(c, (i64)rl * n * zr);
+  if (c.status) return;
+  gemm(c, CMat{envp(c, 0, F_XZ, k), 1, rl}, CMat{znew, (i64)n * zr, 1},
+       Mat{block, (i64)n * zr, 1}, rl, n * zr, zl, 1.0, 0.0);
+  for (i64 e = threadIdx.x; e < (i64)M * cols; e += TTB_THREADS) {
+    const i64 i = e / cols;
+    const int j = (int)(e % cols);
+    enr[e] = (j < rank) ? U[i * p + j] : block[i * zr + (j - rank)];
+  }
+  // padded next core: [S Vh[:rank] @ x_{k+1} ; 0]
+  vfill(padded + (i64)rank * n2 * r2, (i64)zr * n2 * r2, 0.0);
+  double* svh = take(c, (i64)rank * rr);
+  if (c.status) return;
+  for (i64 e = threadIdx.x; e < (i64)rank * rr; e += TTB_THREADS) svh[e] = S[e / rr] * Vh[e];
+  __syncthreads();
+  gemm(c, CMat{svh, rr, 1}, CMat{xcore(c, k + 1), (i64)n2 * r2, 1}, Mat{padded, (i64)n2 * r2, 1},
+       rank, n2 * r2, rr, 1.0, 0.0);
+  const int q = min(M, cols);
+  double* Qb = take(c, (i64)M * q);
+  double* R = take(c, (i64)q * cols);
+  double* nxt = take(c, (i64)q * n2 * r2);
+  if (c.status) return;
+  qr(c, CMat{enr, cols, 1}, M, cols, Mat{Qb, q, 1}, Mat{R, cols, 1});
+  gemm(c, CMat{R, cols, 1}, CMat{padded, (i64)n2 * r2, 1}, Mat{nxt, (i64)n2 * r2, 1}, q, n2 * r2,
+       cols, 1.0, 0.0);
+  int nb = q;
+  const ttb_amen_task_t* T = c.T;
+  if (T->max_rank > 0 && nb > T->max_rank) nb = T->max_rank;  // amen.py:354-358
+  if (nb > c.rmax) {
+    c.status = ST_RANK;
+    return;
+  }
+  double* xk = xcore(c, k);
+  for (i64 e = threadIdx.x; e < (i64)M * nb; e += TTB_THREADS) xk[e] = Qb[(e / nb) * q + e % nb];
+  vcopy(xcore(c, k + 1), nxt, (i64)nb * n2 * r2);
+  __syncthreads();
+  if (threadIdx.x == 0) s->xb[k + 1] = nb;
+  __syncthreads();
+  c.top = mark;
+}
+
+__device__ __noinline__ void backward_update(Ctx& c, int k, const double* u, const double* b_loc,
+                                const double* znew) {
+  Sm* s = c.sm;
+  const int rl = s->xb[k], n = s->n[k], rr = s->xb[k + 1];
+  const int zl = s->zb[k], zr = s->zb[k + 1];
+  const int Kc = n * rr, p = min(rl, Kc);
+  const i64 mark = c.top;
+  double* U = take(c, (i64)rl * p);
+  double* S = take(c, p);
+  double* Vh = take(c, (i64)p * Kc);
+  if (c.status) return;
+  svd(c, CMat{u, Kc, 1}, rl, Kc, Mat{U, p, 1}, S, Mat{Vh, Kc, 1});
+  __syncthreads();
+  const int rank = choose_rank(c, k, u, b_loc, U, S, Vh, rl, Kc, p);
+  if (c.status) return;
+  const int rows = rank + zl;
+  const int rpp = s->xb[k - 1], n0 = s->n[k - 1];
+  double* enr = take(c, (i64)rows * Kc);
+  double* padded = take(c, (i64)rpp * n0 * rows);
+  if (c.status) return;
+  // enriched rows 0..rank-1: Vh[:rank]; rows rank..: z_new (zl*n, zr) @ rxz (zr, rr)
+  vcopy(enr, Vh, (i64)rank * Kc);
+  gemm(c, CMat{znew, zr, 1}, CMat{envp(c, 1, F_XZ, k), rr, 1}, Mat{enr + (i64)rank * Kc, rr, 1},
+       zl * n, rr, zr, 1.0, 0.0);
+  // padded previous core: [x_{k-1} @ (U[:, :rank] S) , 0]
+  {
+    double* us = take(c, (i64)rl * rank);
+    if (c.status) return;
+    for (i64 e = threadIdx.x; e < (i64)rl * rank; e += TTB_THREADS) {
+      i64 i = e / rank, j = e % rank;
+      us[e] = U[i * p + j] * S[j];
+    }
+    for (i64 e = threadIdx.x; e < (i64)rpp * n0; e += TTB_THREADS)
+      for (int j = rank; j < rows; ++j) padded[e * rows + j] = 0.0;
+    __syncthreads();
+    gemm(c, CMat{xcore(c, k - 1), rl, 1}, CMat{us, rank, 1}, Mat{padded, rows, 1}, rpp * n0, rank,
+         rl, 1.0, 0.0);
+  }
+  const int q = min(rows, Kc);
+  double* Qt = take(c, (i64)q * Kc);
+  double* R = take(c, (i64)q * rows);
+  double* prv = take(c, (i64)rpp * n0 * q);
+  if (c.status) return;
+  // QR of enriched^T (Kc x rows): x_k <- Q^T (q, n, rr), x_{k-1} <- padded R^T
+  qr(c, CMat{enr, 1, Kc}, Kc, rows, Mat{Qt, 1, Kc}, Mat{R, rows, 1});
+  gemm(c, CMat{padded, rows, 1}, CMat{R, 1, rows}, Mat{prv, q, 1}, rpp * n0, q, rows, 1.0, 0.0);
+  int nb = q;
+  const ttb_amen_task_t* T = c.T;
+  if (T->max_rank > 0 && nb > T->max_rank) nb = T->max_rank;  // leading rows of x_k stay
+  if (nb > c.rmax) {
+    c.status = ST_RANK;
+    return;
+  }
+  vcopy(xcore(c, k), Qt, (i64)nb * Kc);
+  // x_{k-1} <- prv[:, :nb]
+  double* xp = xcore(c, k - 1);
+  for (i64 e = threadIdx.x; e < (i64)rpp * n0 * nb; e += TTB_THREADS) {
+    i64 i = e / nb, j = e % nb;
+    xp[e] = prv[i * q + j];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s->xb[k] = nb;
+  __syncthreads();
+  c.top = mark;
+}
+
+// ---------------------------------------------------------------------------
+// norms of trains: ||A x - b|| (common.py:118-146) and ||b||
+// ---------------------------------------------------------------------------
+
+// Core i of the residual train A x - b (block sum of the Kronecker core
+// of A x and of -b at b's centre), as (rows, n, cols) row major.
+__device__ __noinline__ void residual_train_core(Ctx& c, int i, double* out, int& rows, int& cols) {
+  Sm* s = c.sm;
+  const int d = c.d;
+  const int n = s->n[i];
+  const int x1 = s->xb[i], x2 = s->xb[i + 1], R2 = s->R[i + 1], rb2 = s->rb[i + 1];
+  const int ra = s->R[i] * x1, ra2 = R2 * x2;  // 1 on the boundaries
+  rows = (i == 0) ? 1 : ra + s->rb[i];
+  cols = (i == d - 1) ? 1 : ra2 + rb2;
+  const int kb = c.T->b_orth_center >= 0 ? c.T->b_orth_center : 0;
+  const double bs = (i == kb) ? -1.0 : 1.0;
+  const double* A = acore(c, i);
+  const double* x = xcore(c, i);
+  const double* b = bcore(c, i);
+  const bool first = (i == 0), last = (i == d - 1);
+  const i64 total = (i64)rows * n * cols;
+  for (i64 e = threadIdx.x; e < total; e += TTB_THREADS) {
+    const int cc = (int)(e % cols);
+    const int j = (int)((e / cols) % n);
+    const int rr = (int)(e / ((i64)cols * n));
+    const bool inA = (first || rr < ra) && (last || cc < ra2);
+    const bool inB = (first || rr >= ra) && (last || cc >= ra2);
+    double v = 0.0;
+    if (inA) {
+      // Kronecker block of A x: rows (a, xr), columns (bb, xc)
+      const int a = rr / x1, xr = rr % x1, bb = cc / x2, xc = cc % x2;
+      for (int l = 0; l < n; ++l)
+        v = fma(A[(((i64)a * n + j) * n + l) * R2 + bb], x[((i64)xr * n + l) * x2 + xc], v);
+    }
+    if (inB) {
+      const int br = first ? 0 : rr - ra, bc = last ? 0 : cc - ra2;
+      v += bs * b[((i64)br * n + j) * rb2 + bc];
+    }
+    out[e] = v;
+  }
+  __syncthreads();
+}
+
+// Frobenius norm of a train given core by core (right QR sweep keeping R).
+// ``which``: 0 = the residual train, 1 = b.
+__device__ __noinline__ double train_norm(Ctx& c, int which) {
+  Sm* s = c.sm;
+  const int d = c.d;
+  const i64 mark = c.top;
+  // largest bond of the train, for the two carry buffers
+  int bmax = 1;
+  for (int i = 0; i <= d; ++i) {
+    const int bnd = which == 0 ? s->R[i] * s->xb[i] + s->rb[i] : s->rb[i];
+    bmax = max(bmax, bnd);
+  }
+  double* carry_a = take(c, (i64)bmax * bmax);
+  double* carry_b = take(c, (i64)bmax * bmax);
+  if (c.status) return 0.0;
+  double* carry = nullptr;
+  int cp = 1;  // columns of the carry
+  for (int i = d - 1; i >= 0; --i) {
+    const i64 imark = c.top;
+    int rows, cols;
+    const int n = s->n[i];
+    const double* core;
+    if (which == 0) {
+      const int ra = s->R[i] * s->xb[i], ra2 = s->R[i + 1] * s->xb[i + 1];
+      const int rr = (i == 0) ? 1 : ra + s->rb[i];
+      const int cc = (i == d - 1) ? 1 : ra2 + s->rb[i + 1];
+      double* buf = take(c, (i64)rr * n * cc);
+      if (c.status) return 0.0;
+      residual_train_core(c, i, buf, rows, cols);
+      core = buf;
+    } else {
+      rows = s->rb[i];
+      cols = s->rb[i + 1];
+      core = bcore(c, i);
+    }
+    const double* m = core;
+    if (carry) {
+      double* mm = take(c, (i64)rows * n * cp);
+      if (c.status) return 0.0;
+      gemm(c, CMat{core, cols, 1}, CMat{carry, cp, 1}, Mat{mm, cp, 1}, rows * n, cp, cols, 1.0,
+           0.0);
+      m = mm;
+    } else {
+      cp = cols;
+    }
+    if (i == 0) {
+      const double nr = vnorm_diff(m, nullptr, (i64)rows * n * cp, s->red);
+      c.top = mark;
+      return nr;
+    }
+    // QR of m^T (n*cp x rows), keep R^T (rows x p) as the next carry
+    const int p = min(n * cp, rows);
+    double* R = take(c, (i64)p * rows);
+    if (c.status) return 0.0;
+    qr(c, CMat{m, 1, (i64)n * cp}, n * cp, rows, Mat{nullptr, 0, 0}, Mat{R, rows, 1});
+    double* nc = (carry == carry_a) ? carry_b : carry_a;
+    for (i64 e = threadIdx.x; e < (i64)rows * p; e += TTB_THREADS) {
+      const i64 a = e / p, q = e % p;
+      nc[e] = R[q * rows + a];
+    }
+    __syncthreads();
+    carry = nc;
+    cp = p;
+    c.top = imark;
+  }
+  c.top = mark;
+  return 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(TTB_THREADS, 1)
+    k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
+  extern __shared__ double pool[];
+  __shared__ Sm sm;
+  const ttb_amen_task_t* T = tasks + blockIdx.x;
+  Ctx c;
+  c.T = T;
+  c.sm = &sm;
+  c.slab = T->slab;
+  c.cap = T->slab_doubles;
+  c.top = 0;
+  c.pool = pool;
+  c.d = T->d;
+  c.rmax = rmax;
+  c.K = T->kickrank;
+  c.status = ST_OK;
+  c.flops = 0.0;
+  c.applies = 0;
+  c.check = 0.0;
+  for (int i = 0; i < PH_N; ++i) c.cyc[i] = 0;
+  long long t_ph = clock64();
+#define PHASE(ph)                         \
+  {                                       \
+    const long long t_now = clock64();    \
+    c.cyc[ph] += t_now - t_ph;            \
+    t_ph = t_now;                         \
+  }
+  const int d = c.d;
+  const int* dims = T->dims;
+  if (d < 2 || d > kD) {
+    if (threadIdx.x == 0) T->result[0] = ST_SETTINGS;
+    return;
+  }
+  // shapes
+  for (int i = threadIdx.x; i <= d; i += TTB_THREADS) {
+    if (i < d) sm.n[i] = dims[i];
+    sm.R[i] = dims[d + i];
+    sm.rb[i] = dims[2 * d + 1 + i];
+    sm.xb[i] = dims[3 * d + 2 + i];
+    sm.zb[i] = dims[4 * d + 3 + i];
+  }
+  __syncthreads();
+  // slots: x cores, z cores, environments
+  if (threadIdx.x == 0) {
+    i64 off = 0;
+    const i64 K = c.K;
+    for (int k = 0; k < d; ++k) {
+      sm.xo[k] = off;
+      off += ((i64)rmax * sm.n[k] * rmax + 31) & ~31LL;
+    }
+    for (int k = 0; k < d; ++k) {
+      sm.zo[k] = off;
+      off += (K * sm.n[k] * K + 31) & ~31LL;
+    }
+    for (int side = 0; side < 2; ++side)
+      for (int k = 0; k < d; ++k) {
+        const int pb = side == 0 ? k : k + 1;
+        const i64 R = sm.R[pb], rb = sm.rb[pb];
+        const i64 sizes[5] = {(i64)rmax * R * rmax, rb * rmax, rb * K, (i64)rmax * R * K,
+                              K * rmax};
+        for (int f = 0; f < 5; ++f) {
+          sm.eo[side][f][k] = off;
+          off += (sizes[f] + 31) & ~31LL;
+        }
+      }
+    sm.flag = (off <= c.cap) ? 1 : 0;
+    sm.stack0 = off;  // the stack starts after the slots
+  }
+  __syncthreads();
+  if (!sm.flag) {
+    if (threadIdx.x == 0) T->result[0] = ST_SLAB;
+    return;
+  }
+  c.top = sm.stack0;
+  __syncthreads();
+  for (int k = 0; k <= d; ++k)
+    if (sm.xb[k] > rmax) {
+      if (threadIdx.x == 0) T->result[0] = ST_RANK;
+      return;
+    }
+  // x0 and z0 into their slots
+  for (int k = 0; k < d; ++k) {
+    vcopy(xcore(c, k), T->x0 + T->x0_off[k], (i64)sm.xb[k] * sm.n[k] * sm.xb[k + 1]);
+    vcopy(zcore(c, k), T->z0 + T->z0_off[k], (i64)sm.zb[k] * sm.n[k] * sm.zb[k + 1]);
+  }
+  __syncthreads();
+  int nsolves = 0, ninexact = 0, sweeps = 0, stop = 2;
+#define CHECK                                  \
+  if (c.status) {                              \
+    if (threadIdx.x == 0) T->result[0] = c.status; \
+    return;                                    \
+  }
+  if (T->x0_orth_center != 0) orth_right(c, true, d - 1);
+  CHECK;
+  orth_right(c, false, d - 1);
+  CHECK;
+  // fit z to b - A x (amen.py:162-224)
+  for (int i = d - 1; i >= 0; --i) {
+    build_env(c, 1, F_ZB, i);
+    build_env(c, 1, F_ZAX, i);
+    CHECK;
+  }
+  const i64 base = c.top;
+  for (int k = 0; k < d - 1; ++k) {
+    build_env(c, 0, F_ZB, k);
+    build_env(c, 0, F_ZAX, k);
+    CHECK;
+    double* core = take(c, (i64)sm.zb[k] * sm.n[k] * sm.zb[k + 1]);
+    CHECK;
+    residual_core(c, k, xcore(c, k), core);
+    z_shift_right(c, k, core, sm.zb[k], sm.n[k], sm.zb[k + 1]);
+    CHECK;
+    c.top = base;
+  }
+  build_env(c, 0, F_ZB, d - 1);
+  build_env(c, 0, F_ZAX, d - 1);
+  for (int k = d - 1; k >= 0; --k) {
+    build_env(c, 1, F_ZB, k);
+    build_env(c, 1, F_ZAX, k);
+    CHECK;
+    double* core = take(c, (i64)sm.zb[k] * sm.n[k] * sm.zb[k + 1]);
+    CHECK;
+    residual_core(c, k, xcore(c, k), core);
+    if (k > 0) {
+      z_shift_left(c, k, core, sm.zb[k], sm.n[k], sm.zb[k + 1]);
+    } else {
+      vcopy(zcore(c, 0), core, (i64)sm.n[0] * sm.zb[1]);
+      __syncthreads();
+    }
+    CHECK;
+    c.top = base;
+  }
+  for (int i = d - 1; i >= 0; --i) {
+    for (int f = 0; f < 5; ++f) build_env(c, 1, f, i);
+    CHECK;
+  }
+  double b_norm = 0.0;
+  if (T->track_residual) {
+    if (T->b_orth_center >= 0) {
+      const int kb = T->b_orth_center;
+      b_norm = vnorm_diff(bcore(c, kb), nullptr, (i64)sm.rb[kb] * sm.n[kb] * sm.rb[kb + 1], sm.red);
+    } else {
+      b_norm = train_norm(c, 1);
+    }
+    CHECK;
+  }
+  double prev_res = 0.0;
+  PHASE(PH_INIT);
+  for (int sweep = 0; sweep < T->max_sweeps; ++sweep) {
+    for (int k = 0; k < d - 1; ++k) {
+      for (int f = 0; f < 5; ++f) build_env(c, 0, f, k);
+      CHECK;
+      PHASE(PH_ENV);
+      const i64 N = (i64)sm.xb[k] * sm.n[k] * sm.xb[k + 1];
+      double* b_loc = take(c, N);
+      double* u = take(c, N);
+      double* znew = take(c, (i64)sm.zb[k] * sm.n[k] * sm.zb[k + 1]);
+      CHECK;
+      project(c, envp(c, 0, F_B, k), sm.rb[k], sm.xb[k], bcore(c, k), sm.n[k], sm.rb[k + 1],
+              envp(c, 1, F_B, k), sm.xb[k + 1], b_loc, 1.0, 0.0);
+      solve_local(c, k, b_loc, u, &nsolves, &ninexact);
+      CHECK;
+      PHASE(PH_SOLVE);
+      residual_core(c, k, u, znew);
+      PHASE(PH_ZCORE);
+      forward_update(c, k, u, b_loc, znew);
+      CHECK;
+      z_shift_right(c, k, znew, sm.zb[k], sm.n[k], sm.zb[k + 1]);
+      CHECK;
+      PHASE(PH_TRUNC);
+      c.top = base;
+    }
+    for (int f = 0; f < 5; ++f) build_env(c, 0, f, d - 1);
+    CHECK;
+    for (int k = d - 1; k >= 0; --k) {
+      for (int f = 0; f < 5; ++f) build_env(c, 1, f, k);
+      CHECK;
+      PHASE(PH_ENV);
+      const i64 N = (i64)sm.xb[k] * sm.n[k] * sm.xb[k + 1];
+      double* b_loc = take(c, N);
+      double* u = take(c, N);
+      double* znew = take(c, (i64)sm.zb[k] * sm.n[k] * sm.zb[k + 1]);
+      CHECK;
+      project(c, envp(c, 0, F_B, k), sm.rb[k], sm.xb[k], bcore(c, k), sm.n[k], sm.rb[k + 1],
+              envp(c, 1, F_B, k), sm.xb[k + 1], b_loc, 1.0, 0.0);
+      solve_local(c, k, b_loc, u, &nsolves, &ninexact);
+      CHECK;
+      PHASE(PH_SOLVE);
+      residual_core(c, k, u, znew);
+      PHASE(PH_ZCORE);
+      if (k == 0) {
+        vcopy(xcore(c, 0), u, N);
+        vcopy(zcore(c, 0), znew, (i64)sm.n[0] * sm.zb[1]);
+        __syncthreads();
+      } else {
+        backward_update(c, k, u, b_loc, znew);
+        CHECK;
+        z_shift_left(c, k, znew, sm.zb[k], sm.n[k], sm.zb[k + 1]);
+        CHECK;
+      }
+      PHASE(PH_TRUNC);
+      c.top = base;
+    }
+    sweeps = sweep + 1;
+    {
+      int mb = 1;
+      for (int k = 0; k <= d; ++k) mb = max(mb, sm.xb[k]);
+      if (threadIdx.x == 0) T->residuals[T->max_sweeps + sweep] = (double)mb;
+    }
+    if (!T->track_residual) continue;
+    const double rn = train_norm(c, 0);
+    CHECK;
+    PHASE(PH_RESID);
+    const double res = (b_norm == 0.0) ? rn : rn / b_norm;
+    if (threadIdx.x == 0) T->residuals[sweep] = res;
+    if (T->residual_mode && res <= T->residual_tol) {
+      stop = 0;
+      break;
+    }
+    if (T->stagnation_on && sweep >= 1 && res > T->stagnation_factor * prev_res) {
+      stop = 1;
+      break;
+    }
+    prev_res = res;
+  }
+  // amen.py:710-720: bonds above the product of the modes on their left
+  {
+    int last = 0;
+    double prod = 1.0;
+    for (int k = 1; k < d; ++k) {
+      prod *= sm.n[k - 1];
+      if ((double)sm.xb[k] > prod) last = k;
+    }
+    if (last > 0) {
+      orth_left(c, last);
+      CHECK;
+      orth_right(c, true, last);
+      CHECK;
+    }
+  }
+  if (threadIdx.x == 0) {
+    T->result[0] = ST_OK;
+    T->result[1] = sweeps;
+    T->result[2] = stop;
+    T->result[3] = nsolves;
+    T->result[4] = ninexact;
+    for (int k = 0; k <= d; ++k) T->result[5 + k] = sm.xb[k];
+    for (int k = 0; k < d; ++k) T->x_offsets[k] = sm.xo[k];
+    T->residuals[2 * T->max_sweeps] = c.flops;
+    T->residuals[2 * T->max_sweeps + 1] = (double)c.applies;
+    for (int i = 0; i < PH_N; ++i) T->residuals[2 * T->max_sweeps + 2 + i] = (double)c.cyc[i];
+    T->residuals[2 * T->max_sweeps + 2 + PH_N] = c.check;
+  }
+#undef PHASE
+#undef CHECK
+}
+
+}  // namespace
+
+extern "C" {
+
+long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
+                                int direct_solve_size) {
+  if (d < 2 || d > kD) return -1;
+  const long long K = kickrank;
+  long long slots = 0, nmax = 1, Rmax = 1, rbmax = 1;
+  for (int k = 0; k < d; ++k) {
+    const long long n = dims[k];
+    nmax = std::max(nmax, n);
+    slots += ((long long)rmax * n * rmax + 31) & ~31LL;
+    slots += (K * n * K + 31) & ~31LL;
+  }
+  for (int k = 0; k <= d; ++k) {
+    Rmax = std::max<long long>(Rmax, dims[d + k]);
+    rbmax = std::max<long long>(rbmax, dims[2 * d + 1 + k]);
+  }
+  for (int side = 0; side < 2; ++side)
+    for (int k = 0; k < d; ++k) {
+      const int pb = side == 0 ? k : k + 1;
+      const long long R = dims[d + pb], rb = dims[2 * d + 1 + pb];
+      const long long sizes[5] = {(long long)rmax * R * rmax, rb * rmax, rb * K,
+                                  (long long)rmax * R * K, K * rmax};
+      for (int f = 0; f < 5; ++f) slots += (sizes[f] + 31) & ~31LL;
+    }
+  // stack bound of one sweep step: b_loc, u and z_new, then the largest of
+  // the sub-steps, each term rounded up generously
+  const long long r = rmax, n = nmax, R = Rmax, N = r * n * r, cols = r + K;
+  const long long env = 2 * r * R * n * r + r * n * r;
+  const long long apply = 2 * r * n * R * r;
+  const long long dn = std::min<long long>(direct_solve_size, N);
+  const long long direct = dn * dn + dn;
+  const long long iter = N + 7 * N + apply;
+  const long long rank = 3 * N + apply;
+  const long long fact = r * n * r + r + r * n * r        // U S Vh
+                         + (r * n) * r + 2 * r * r + 4 * r  // svd work
+                         + (r * n) * cols + 2 * cols * n * r + r * r  // enriched, padded, svh
+                         + r * n * cols + cols * cols + cols * n * r  // Q, R, next
+                         + r * n * cols + cols + r * n * K;            // qr work, block
+  const long long bb = R * r + rbmax;
+  const long long resid = 2 * bb * bb + bb * n * bb + bb * n * bb + bb * bb;
+  const long long step = 3 * N + K * n * K +
+                         std::max({env, direct, iter, rank + fact, resid, 2 * rbmax * n * r});
+  return slots + 2 * step + (1 << 16);
+}
+
+int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream) {
+  if (count <= 0) return 0;
+  static int configured = 0;
+  const size_t smem = kPoolBytes;
+  if (!configured) {
+    cudaFuncSetAttribute(k_amen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = 1;
+  }
+  k_amen<<<count, TTB_THREADS, smem, reinterpret_cast<cudaStream_t>(stream)>>>(tasks, rmax);
+  return (int)cudaGetLastError();
+}
+
+}  // extern "C"

@@ -26,7 +26,7 @@ typedef long long i64;
 // reductions
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double warp_sum(double v) {
+static __device__ __forceinline__ double warp_sum(double v) {
   // tree towards lane 0, then broadcast lane 0 so all lanes agree bitwise
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   return __shfl_sync(0xffffffffu, v, 0);
@@ -34,7 +34,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Sum over the block; every thread returns the same value.  ``red`` must
 // hold TTB_WARPS doubles of shared memory.  Contains two __syncthreads.
-__device__ __forceinline__ double block_sum(double v, double* red) {
+static __device__ __forceinline__ double block_sum(double v, double* red) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   v = warp_sum(v);
   __syncthreads();
@@ -48,7 +48,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 
 // Index of the entry of largest absolute value, first index on ties (the
 // LAPACK idamax convention).  ``redv``/``redi`` hold TTB_WARPS entries.
-__device__ __forceinline__ int block_argmax_abs(double v, int idx, double* redv, int* redi) {
+static __device__ __forceinline__ int block_argmax_abs(double v, int idx, double* redv, int* redi) {
   double a = (idx >= 0) ? fabs(v) : -1.0;
   int i = idx;
   for (int o = 16; o > 0; o >>= 1) {
@@ -100,7 +100,7 @@ struct GemmSmem {
 // C[m0:m0+64, n0:n0+64] = alpha * A * B + beta * C over the full K range.
 // A is M x K, B is K x N.  beta == 0 never reads C.  Thread (tx, ty) of a
 // 16 x 16 grid owns rows ty + 16 i and columns tx + 16 j.
-__device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0, int n0,
+static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0, int n0,
                               double alpha, double beta, GemmSmem& sm) {
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
@@ -177,7 +177,7 @@ __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0
 }
 
 // Whole product, looping over all output tiles with the one block.
-__device__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
+static __device__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
                          GemmSmem& sm) {
   for (int m0 = 0; m0 < M; m0 += GBM)
     for (int n0 = 0; n0 < N; n0 += GBN) cta_gemm_tile(A, B, C, M, N, K, m0, n0, alpha, beta, sm);
@@ -187,7 +187,7 @@ __device__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alph
 // copies
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void cta_copy(CMat src, Mat dst, int M, int N, double alpha = 1.0) {
+static __device__ __forceinline__ void cta_copy(CMat src, Mat dst, int M, int N, double alpha = 1.0) {
   const int total = M * N;
   // walk the unit-stride direction of the destination when there is one
   const bool rowfast = (dst.cs == 1);
@@ -198,7 +198,7 @@ __device__ __forceinline__ void cta_copy(CMat src, Mat dst, int M, int N, double
   }
 }
 
-__device__ __forceinline__ void cta_fill(Mat dst, int M, int N, double v) {
+static __device__ __forceinline__ void cta_fill(Mat dst, int M, int N, double v) {
   const int total = M * N;
   for (int e = threadIdx.x; e < total; e += TTB_THREADS) {
     int i = e % M, j = e / M;
@@ -217,7 +217,7 @@ __device__ __forceinline__ void cta_fill(Mat dst, int M, int N, double v) {
 // H = I - tau v v^T built as in dlarfg: beta = -sign(alpha) ||x||,
 // tau = (beta - alpha) / beta, v = x / (alpha - beta); a column whose
 // sub-diagonal part is exactly zero gets tau = 0.
-__device__ void cta_householder(double* W, int m, int k, i64 ldw, double* tau, double* red) {
+static __device__ void cta_householder(double* W, int m, int k, i64 ldw, double* tau, double* red) {
   const int p = m < k ? m : k;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int j = 0; j < p; ++j) {
@@ -260,7 +260,7 @@ __device__ void cta_householder(double* W, int m, int k, i64 ldw, double* tau, d
 
 // Overwrite the m x q matrix X (strided) with H_0 H_1 ... H_{p-1} X, the
 // reflectors of cta_householder (applied last to first).
-__device__ void cta_apply_q(const double* W, int m, int p, i64 ldw, const double* tau, Mat X,
+static __device__ void cta_apply_q(const double* W, int m, int p, i64 ldw, const double* tau, Mat X,
                             int q) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int j = p - 1; j >= 0; --j) {
@@ -284,7 +284,7 @@ __device__ void cta_apply_q(const double* W, int m, int p, i64 ldw, const double
 // (p x k), p = min(m, k).  ``W`` is an m x k column-major work area (unit
 // row step, column step m), ``tau`` p doubles; both may be shared or
 // global memory.  Q and R may be NULL to skip them.
-__device__ void cta_qr(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R, double* red) {
+static __device__ void cta_qr(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R, double* red) {
   const int p = m < k ? m : k;
   cta_copy(A, Mat{W, 1, (i64)m}, m, k);
   __syncthreads();
@@ -318,7 +318,7 @@ __device__ void cta_qr(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat 
 // |b_p . b_q| > tol sqrt(|b_p|^2 |b_q|^2); sweeps stop when one sweep
 // rotates nothing, or after ``max_sweeps``.  Returns the sweeps used, or -1
 // when the cap was hit.
-__device__ int cta_jacobi(double* B, int k, i64 ldb, double* V, i64 ldv, int max_sweeps,
+static __device__ int cta_jacobi(double* B, int k, i64 ldb, double* V, i64 ldv, int max_sweeps,
                           double tol, int* flag) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < k * k; e += TTB_THREADS) {
@@ -393,7 +393,7 @@ __device__ int cta_jacobi(double* B, int k, i64 ldb, double* V, i64 ldv, int max
 // order (k ints), flag (1 int).  U (m x k), S (k) and Vh (k x k) are
 // strided outputs; U is also used as the work area of the final Q product.
 // Returns the Jacobi sweeps used, or -1 if the sweep cap was hit.
-__device__ int cta_svd_tall(CMat A, int m, int k, double* W, double* tau, double* Bsq, double* V,
+static __device__ int cta_svd_tall(CMat A, int m, int k, double* W, double* tau, double* Bsq, double* V,
                             double* sv, int* order, int* flag, Mat U, double* S, Mat Vh,
                             double* red) {
   cta_copy(A, Mat{W, 1, (i64)m}, m, k);
@@ -447,7 +447,7 @@ __device__ int cta_svd_tall(CMat A, int m, int k, double* W, double* tau, double
 // leading dimension ld, then back substitution.  b is overwritten with the
 // solution and W with the factors.  Returns 0, or the 1-based index of the
 // first exactly-zero pivot (the solve then stops, like gesv's info > 0).
-__device__ int cta_gepp_solve(double* W, i64 ld, double* b, int n, double* redv, int* redi) {
+static __device__ int cta_gepp_solve(double* W, i64 ld, double* b, int n, double* redv, int* redi) {
   for (int j = 0; j < n; ++j) {
     double best = -1.0;
     int bi = -1;
@@ -505,7 +505,7 @@ constexpr int YCH = 512;  // columns per chunk of the blocked trailing updates
 // major, leading dimension ld), panels of LNB columns factored in ``panel``
 // (rows x LNB doubles, shared or global memory), trailing updates as GEMMs.
 // Same pivot rule and result as cta_gepp_solve; b becomes the solution.
-__device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, double* panel, double* redv,
+static __device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, double* panel, double* redv,
                                 int* redi, int* ipiv, GemmSmem& gsm) {
   const int tid = threadIdx.x;
   for (int j0 = 0; j0 < n; j0 += LNB) {
@@ -599,7 +599,7 @@ __device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, double* pan
 // reflector H_0 ... H_{jb-1} = I - V T V^T, V the rows x jb explicit
 // reflector block (unit diagonal, zeros above) in Wp with leading dim ldw
 // (LAPACK dlarft, forward column-wise).  G is jb x jb scratch.
-__device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, const double* tau,
+static __device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, const double* tau,
                             double* G, double* Tm, GemmSmem& gsm) {
   cta_gemm(CMat{Wp, ldw, 1}, CMat{Wp, 1, ldw}, Mat{G, 1, LNB}, jb, jb, rows, 1.0, 0.0, gsm);
   if (threadIdx.x == 0) {
@@ -620,7 +620,7 @@ __device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, const d
 // W by cta_qr_blocked (explicit reflector blocks, leading dimension m),
 // applied last block first; only rows >= the block's first row change.
 // Columns of X left of a block are untouched (as for an identity start).
-__device__ void cta_apply_q_blocked(const double* W, int m, int p, const double* tau, Mat X,
+static __device__ void cta_apply_q_blocked(const double* W, int m, int p, const double* tau, Mat X,
                                     int nx, double* Y, double* G, double* Tm, GemmSmem& gsm) {
   const int tid = threadIdx.x;
   const int last = ((p - 1) / LNB) * LNB;
@@ -655,7 +655,7 @@ __device__ void cta_apply_q_blocked(const double* W, int m, int p, const double*
 // C -= V (T^T (V^T C)) as two GEMMs through Y (LNB x k, shared).  Q (m x p)
 // and R (p x k) as in cta_qr; either may be NULL.  Same reflectors and R as
 // the unblocked factorisation up to rounding.
-__device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R,
+static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R,
                                double* Y, double* G, double* Tm, double* red, GemmSmem& gsm) {
   const int p = m < k ? m : k;
   const int tid = threadIdx.x;
@@ -721,7 +721,7 @@ __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* tau, Mat
 // into the global work area W, Jacobi on R in Bsq/V (global or shared), U
 // by the blocked reflector product.  Y needs LNB * max(k, 1) doubles, G and
 // Tm LNB * LNB each (shared).
-__device__ int cta_svd_tall_blocked(CMat A, int m, int k, double* W, double* tau, double* Bsq,
+static __device__ int cta_svd_tall_blocked(CMat A, int m, int k, double* W, double* tau, double* Bsq,
                                     double* V, double* sv, int* order, int* flag, Mat U, double* S,
                                     Mat Vh, double* Y, double* G, double* Tm, double* red,
                                     GemmSmem& gsm) {

@@ -1,0 +1,304 @@
+"""Many AMEn solves in one persistent launch (``ttb_amen_persistent``).
+
+Each request becomes one thread block that runs the whole solve on the
+device (``csrc/ttb_amen.cu``).  The host packs every request's operator,
+right-hand side, initial guess and random residual start into a few large
+buffers (one host-to-device copy), builds the task table, launches once and
+reads back the bonds, stop reasons and residual histories.  A solve whose
+bonds outgrow the slot capacity ``rmax`` is re-run with a larger one.
+
+Argument semantics, validation and the ``SolverInfo`` produced are those of
+``amen`` (``ttnumpy/solvers/amen.py:395-725``); MINRES (``symmetric=True``)
+or direct local solves only -- GMRES requests belong to the lockstep engine.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import kernels as K
+from . import tensor_train
+from ._lib import check
+from .solvers.common import (
+    LocalSolver,
+    SolverInfo,
+    StopReason,
+    TruncationMode,
+    _SolverSettings,
+)
+from .tensor_train import TensorTrain
+
+P, I, L, D = C.c_void_p, C.c_int, C.c_longlong, C.c_double
+
+
+Task = _lib.AmenTask
+
+
+def _lib_handle():
+    return K.lib()
+
+
+def _host_cores(t) -> List[np.ndarray]:
+    if isinstance(t, TensorTrain):
+        return t.to_numpy()
+    return [np.asarray(c, dtype=np.float64).reshape(c.shape if c.ndim == 4 else
+                                                    (c.shape[0], c.shape[1], 1, c.shape[2]))
+            for c in t]
+
+
+def _orth(t) -> Optional[int]:
+    return t.orth_center if isinstance(t, TensorTrain) else None
+
+
+STATUS = {0: "ok", -1: "singular local system", -3: "slab too small", -4: "rank above rmax",
+          -5: "unsupported settings"}
+
+
+@dataclass
+class Result:
+    x: Optional[TensorTrain]
+    info: SolverInfo
+    status: int
+
+
+class _Prepared:
+    """One request's host data and resolved settings."""
+
+    def __init__(self, A, b, x0, kwargs):
+        kw = dict(kwargs)
+        kick = kw.pop("kickrank", 4)
+        eth = kw.pop("error_threshold", 1e-7)
+        max_rank = kw.pop("max_rank", None)
+        damp = kw.pop("residual_damp", 2.0)
+        seed = kw.pop("seed", None)
+        return_info = kw.pop("return_info", True)
+        kw.pop("inplace", None)
+        if kick <= 0:
+            raise ValueError(f"kickrank must be a positive integer, got {kick}")
+        if max_rank is not None and max_rank <= 0:
+            raise ValueError(f"max_rank must be a positive integer, got {max_rank}")
+        if damp < 1.0:
+            raise ValueError(f"residual_damp must be >= 1, got {damp}")
+        self.A = _host_cores(A)
+        self.b = _host_cores(b)
+        d = len(self.A)
+        st = _SolverSettings.resolve(
+            max_sweeps=kw.pop("max_sweeps", 1), residual_tol=kw.pop("residual_tol", None),
+            stagnation_factor=kw.pop("stagnation_factor", "auto"),
+            local_solver=kw.pop("local_solver", "auto"), symmetric=kw.pop("symmetric", False),
+            direct_solve_size=kw.pop("direct_solve_size", 1000), return_info=return_info,
+            local_rtol=kw.pop("local_rtol", None),
+            allow_dense_fallback=kw.pop("allow_dense_fallback", False),
+            truncation_steps=max(2 * (d - 1), 1))
+        if kw:
+            raise TypeError(f"unexpected arguments {sorted(kw)}")
+        if st.allow_dense_fallback:
+            raise ValueError("the persistent path has no dense fallback for local solves")
+        modes = [c.shape[1] for c in self.b]
+        if [c.shape[1] for c in self.A] != modes or [c.shape[2] for c in self.A] != modes:
+            raise tensor_train.DimensionMismatch("operator and right-hand side modes differ")
+        if x0 is None:
+            ranks = [c.shape[0] for c in self.b] + [1]
+            self.x0 = [np.ones((ranks[i], modes[i], 1, ranks[i + 1])) for i in range(d)]
+            self.x0_oc = -1
+        else:
+            self.x0 = _host_cores(x0)
+            oc = _orth(x0)
+            self.x0_oc = -1 if oc is None else oc
+        rng = np.random.default_rng(seed)
+        zr = [1] + [kick] * (d - 1) + [1]
+        self.z0 = [rng.random((zr[i], modes[i], 1, zr[i + 1])) for i in range(d)]
+        self.b_oc = _orth(b)
+        self.st, self.kick, self.eth, self.max_rank, self.damp = st, kick, eth, max_rank, damp
+        self.d = d
+        self.modes = modes
+
+    def dims(self) -> np.ndarray:
+        d = self.d
+        R = [c.shape[0] for c in self.A] + [1]
+        rb = [c.shape[0] for c in self.b] + [1]
+        xb = [c.shape[0] for c in self.x0] + [1]
+        zb = [c.shape[0] for c in self.z0] + [1]
+        return np.array(self.modes + R + rb + xb + zb, dtype=np.int32)
+
+
+class PersistentBatch:
+    """Requests packed on the device for the persistent kernel.
+
+    Construction packs the inputs (one host-to-device copy), sizes and
+    allocates the slabs and uploads the task table; :meth:`run` launches the
+    kernel and returns the results.  The inputs are read-only to the kernel,
+    so a batch can be run again.
+    """
+
+    def __init__(self, preps: List["_Prepared"], rmax: int, debug: bool = False):
+        lib = _lib_handle()
+        self.preps, self.rmax = preps, rmax
+        n = len(preps)
+        blocks, offs = [], []
+        pos = 0
+        for p in preps:
+            for cores in (p.A, p.b, p.x0, p.z0):
+                for c in cores:
+                    offs.append(pos)
+                    blocks.append(c.reshape(-1))
+                    pos += c.size
+        host = np.concatenate(blocks) if blocks else np.zeros(1)
+        self.h2d_bytes = host.nbytes
+        self.dev_in = torch.from_numpy(host).pin_memory().to("cuda", non_blocking=True)
+        self.dev_off = torch.from_numpy(np.asarray(offs, dtype=np.int64)).to("cuda")
+        dims_host = [p.dims() for p in preps]
+        dim_pos = np.cumsum([0] + [len(x) for x in dims_host])
+        self.dev_dims = torch.from_numpy(np.concatenate(dims_host)).to("cuda")
+        sizes = []
+        for p, dh in zip(preps, dims_host):
+            arr = (C.c_int * len(dh))(*dh.tolist())
+            size = lib.ttb_amen_slab_doubles(p.d, arr, p.kick, rmax,
+                                             int(min(p.st.direct_solve_size, 1 << 30)))
+            if size < 0:
+                raise ValueError("train too long for the persistent path")
+            sizes.append((size + 63) // 64 * 64)
+        self.slab_pos = np.cumsum([0] + sizes)
+        self.slabs = torch.empty(int(self.slab_pos[-1]), dtype=torch.float64, device="cuda")
+        self.dmax = max(p.d for p in preps)
+        smax = max(max(p.st.max_sweeps for p in preps), 1)
+        self.resid = torch.zeros(n, 2 * smax + 12, dtype=torch.float64, device="cuda")
+        self.result = torch.zeros(n, 6 + self.dmax, dtype=torch.int32, device="cuda")
+        self.xoff = torch.zeros(n, self.dmax, dtype=torch.int64, device="cuda")
+        tasks = (Task * n)()
+        base_in, base_off = self.dev_in.data_ptr(), self.dev_off.data_ptr()
+        opos = 0
+        for i, p in enumerate(preps):
+            t = tasks[i]
+            ptrs = []
+            for _ in range(4):
+                ptrs.append(base_off + 8 * opos)
+                opos += p.d
+            t.A = t.b = t.x0 = t.z0 = base_in
+            t.A_off, t.b_off, t.x0_off, t.z0_off = ptrs
+            t.dims = self.dev_dims.data_ptr() + 4 * int(dim_pos[i])
+            t.slab = self.slabs.data_ptr() + 8 * int(self.slab_pos[i])
+            t.slab_doubles = sizes[i]
+            t.residuals = self.resid[i].data_ptr()
+            t.result = self.result[i].data_ptr()
+            t.x_offsets = self.xoff[i].data_ptr()
+            st = p.st
+            t.d, t.kickrank = p.d, p.kick
+            t.max_rank = p.max_rank or 0
+            t.max_sweeps = st.max_sweeps
+            t.direct_solve_size = (int(min(st.direct_solve_size, 1 << 30))
+                                   if st.iterative_solver is not None else (1 << 30))
+            t.track_residual = int(st.track_residual)
+            t.residual_mode = int(st.truncation_mode is TruncationMode.RESIDUAL)
+            t.stagnation_on = int(st.stagnation_factor is not None)
+            t.x0_orth_center = p.x0_oc
+            t.b_orth_center = -1 if p.b_oc is None else p.b_oc
+            t.residual_tol = st.residual_tol or 0.0
+            t.error_threshold = p.eth
+            t.residual_damp = p.damp
+            t.stagnation_factor = st.stagnation_factor or 0.0
+            # MINRES tolerance; GMRES-only settings refuse iterative local solves
+            t.local_rtol = ((st.local_rtol or 0.0) if st.iterative_solver is LocalSolver.MINRES
+                            else -1.0)
+            t.truncation_tol = st.truncation_tol or 0.0
+            t.debug = int(debug)
+        raw = np.frombuffer(bytes(tasks), dtype=np.uint8)
+        self.dev_tasks = torch.from_numpy(raw.copy()).to("cuda")
+
+    def launch(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Queue the kernel on ``stream`` (asynchronous)."""
+        s = stream or torch.cuda.current_stream()
+        check(K.lib().ttb_amen_persistent(C.c_void_p(self.dev_tasks.data_ptr()),
+                                          len(self.preps), self.rmax, C.c_void_p(s.cuda_stream)),
+              "ttb_amen_persistent")
+
+    def gemm_flops(self) -> float:
+        """FP64 FLOPs of the dense products of the last launch, all blocks."""
+        resid_h = self.resid.cpu().numpy()
+        return float(sum(resid_h[i, 2 * p.st.max_sweeps] for i, p in enumerate(self.preps)))
+
+    PHASES = ("env", "solve", "zcore", "trunc_enrich", "enrich", "resid", "init")
+
+    def breakdown(self):
+        """Per solve: operator applications and SM cycles per phase of the
+        last launch (environment updates, local solves, residual cores,
+        truncation with enrichment, residual checks, set-up)."""
+        resid_h = self.resid.cpu().numpy()
+        out = []
+        for i, p in enumerate(self.preps):
+            base = 2 * p.st.max_sweeps
+            row = {"applies": int(resid_h[i, base + 1])}
+            for j, name in enumerate(self.PHASES):
+                row[name] = float(resid_h[i, base + 2 + j])
+            row["check"] = float(resid_h[i, base + 9])
+            out.append(row)
+        return out
+
+    def collect(self) -> List[Result]:
+        """Results of the last launch (synchronises with it)."""
+        res_h = self.result.cpu().numpy()
+        resid_h = self.resid.cpu().numpy()
+        xoff_h = self.xoff.cpu().numpy()
+        out = []
+        for i, p in enumerate(self.preps):
+            status = int(res_h[i, 0])
+            info = SolverInfo()
+            if status != 0:
+                out.append(Result(None, info, status))
+                continue
+            sweeps = int(res_h[i, 1])
+            info.num_sweeps_run = sweeps
+            info.stop_reason = [StopReason.CONVERGED, StopReason.STAGNATED,
+                                StopReason.MAX_SWEEPS][int(res_h[i, 2])]
+            info.local_solves = int(res_h[i, 3])
+            info.local_inexact = int(res_h[i, 4])
+            if p.st.track_residual:
+                info.residuals = [float(v) for v in resid_h[i, :sweeps]]
+            ms = p.st.max_sweeps
+            info.max_bonds = [int(v) for v in resid_h[i, ms:ms + sweeps]]
+            bonds = [int(v) for v in res_h[i, 5:6 + p.d]]
+            base = int(self.slab_pos[i])
+            cores = []
+            for k in range(p.d):
+                o = base + int(xoff_h[i, k])
+                size = bonds[k] * p.modes[k] * bonds[k + 1]
+                cores.append(self.slabs[o:o + size].view(bonds[k], p.modes[k], 1,
+                                                         bonds[k + 1]).clone())
+            out.append(Result(TensorTrain._wrap(cores, orth_center=0), info, status))
+        return out
+
+    def run(self, stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
+        self.launch(stream)
+        return self.collect()
+
+
+def prepare(requests: Sequence) -> List["_Prepared"]:
+    """Validate and resolve ``[(A, b, x0, kwargs), ...]`` on the host."""
+    return [_Prepared(A, b, x0, kw) for A, b, x0, kw in requests]
+
+
+def amen_persistent(requests: Sequence, rmax: int = 64, max_rmax: int = 256,
+                    stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
+    """Solve ``[(A, b, x0, kwargs), ...]`` in one persistent launch; solves
+    whose bonds outgrow ``rmax`` are re-run with twice the capacity."""
+    K.device_ok()
+    preps = prepare(requests)
+    results: List[Optional[Result]] = [None] * len(preps)
+    todo = list(range(len(preps)))
+    while todo:
+        out = PersistentBatch([preps[i] for i in todo], rmax).run(stream)
+        retry = []
+        for i, res in zip(todo, out):
+            if res.status == -4 and rmax < max_rmax:
+                retry.append(i)
+            else:
+                results[i] = res
+        todo = retry
+        rmax = min(2 * rmax, max_rmax)
+    return results
