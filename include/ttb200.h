@@ -169,6 +169,30 @@ typedef struct {
 long long ttb_qr_work_doubles(int m, int k);
 int ttb_qr(const ttb_qr_t* problems, int count, void* stream);
 
+/* ttb_qr for callers that cannot allocate device memory (no counterpart in
+ * the reference).  Same factorisation and results as ttb_qr; the ``work``
+ * field is ignored and the work areas come from one fixed array of
+ * TTB_QR_STATIC_DOUBLES doubles (16 MiB) inside the library.  It is meant
+ * for a caller whose device memory is all owned by another allocator it may
+ * not call into (a serving process that reserved its HBM up front, a
+ * host-language binding that holds only its input and output buffers), or
+ * that must not take the implicit device synchronisation of
+ * cudaMalloc/cudaFree.
+ *
+ * Limit: the problems of one call that do not fit in shared memory
+ * (8 * (m*k + min(m, k)) bytes above 200 KiB) need
+ * m*k + min(m, k) doubles each, rounded up to 32, and together at most
+ * TTB_QR_STATIC_DOUBLES; a call over the limit launches nothing and
+ * returns TTB_ERR_STATIC_SCRATCH.  Nothing in the array must start at zero.
+ * The array is shared by every call on a device: calls that overlap in time
+ * (on different streams or host threads) race and must be serialised by the
+ * caller.  The first call on each device, made with that device current,
+ * looks up the array's address (count = 0 is enough); make it before any
+ * stream capture begins on that device. */
+#define TTB_QR_STATIC_DOUBLES 2097152
+#define TTB_ERR_STATIC_SCRATCH (-2)
+int ttb_qr_static(const ttb_qr_t* problems, int count, void* stream);
+
 /* ------------------------------------------------------------------------
  * Thin SVD of an m x k strided matrix, a = u diag(s) vh with s descending,
  * p = min(m, k): u (m x p), s (p), vh (p x k).  Householder QR followed by

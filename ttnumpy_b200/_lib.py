@@ -128,6 +128,7 @@ _SIGNATURES = {
     "ttb_project": ([C.POINTER(Project), I, P], I),
     "ttb_qr_work_doubles": ([I, I], L),
     "ttb_qr": ([C.POINTER(QR), I, P], I),
+    "ttb_qr_static": ([C.POINTER(QR), I, P], I),
     "ttb_svd_work_doubles": ([I, I], L),
     "ttb_svd": ([C.POINTER(SVD), I, P], I),
     "ttb_lu_work_doubles": ([I], L),

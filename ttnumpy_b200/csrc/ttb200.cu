@@ -1300,6 +1300,46 @@ __global__ void __launch_bounds__(TTB_THREADS) k_fma_peak(double* out, int iters
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Fixed scratch for ttb_qr_static: one array in the module's own device
+// memory (it exists on every device the module is loaded on), so the entry
+// point needs no allocator.  Nothing in it has to start at zero: the blocked
+// factorisation copies the input into its slice and writes every tau before
+// reading it.  Calls that overlap in time (other streams, other host
+// threads) share it and race; they must be serialised by the caller.
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) double g_qr_static[TTB_QR_STATIC_DOUBLES];
+
+namespace {
+
+constexpr int kStaticDevices = 64;
+constexpr i64 kStaticAlign = 32;  // doubles: every slice starts on 256 bytes
+std::atomic<double*> g_qr_static_base[kStaticDevices];
+
+// Device address of g_qr_static on the current device, looked up on the
+// first call there (with that device current) and kept.
+int qr_static_base(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= kStaticDevices) return (int)cudaErrorInvalidDevice;
+  double* p = g_qr_static_base[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void* addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_qr_static);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaFuncSetAttribute(k_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap);
+    if (e != cudaSuccess) return (int)e;
+    p = static_cast<double*>(addr);
+    g_qr_static_base[dev].store(p, std::memory_order_release);
+  }
+  *out = p;
+  return 0;
+}
+
+}  // namespace
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -1448,6 +1488,47 @@ int ttb_qr(const ttb_qr_t* ps, int count, void* stream) {
     ProfScope ps(P_QR, s, fl, 0.0);
     k_qr<<<qb.count, TTB_THREADS, (size_t)smem, s>>>(qb);
     counted();
+  }
+  return last_error();
+}
+
+int ttb_qr_static(const ttb_qr_t* ps, int count, void* stream) {
+  double* base = nullptr;
+  int e = qr_static_base(&base);
+  if (e) return e;
+  if (count <= 0) return 0;
+  // pass 0 checks every problem before anything is launched; pass 1 gives
+  // each blocked problem its own slice (in call order) and launches
+  for (int pass = 0; pass < 2; ++pass) {
+    i64 used = 0;
+    for (int i0 = 0; i0 < count; i0 += kMaxQ) {
+      QBatch qb;
+      qb.count = std::min(kMaxQ, count - i0);
+      i64 smem = 0;
+      for (int j = 0; j < qb.count; ++j) {
+        qb.d[j] = ps[i0 + j];
+        const i64 whole = qr_need(qb.d[j].m, qb.d[j].k) * 8;
+        if (whole <= kSmemCap) {
+          qb.mode[j] = 0;
+          qb.d[j].work = nullptr;
+          smem = std::max(smem, whole);
+        } else {
+          const i64 blk = blocked_smem(qb.d[j].k) * 8;
+          if (blk > kSmemCap) return (int)cudaErrorInvalidValue;
+          const i64 need = (qr_need(qb.d[j].m, qb.d[j].k) + kStaticAlign - 1) / kStaticAlign *
+                           kStaticAlign;
+          if (need > TTB_QR_STATIC_DOUBLES - used) return TTB_ERR_STATIC_SCRATCH;
+          qb.mode[j] = 1;
+          qb.d[j].work = base + used;
+          used += need;
+          smem = std::max(smem, blk);
+        }
+      }
+      if (pass == 1) {
+        k_qr<<<qb.count, TTB_THREADS, (size_t)smem, as_stream(stream)>>>(qb);
+        counted();
+      }
+    }
   }
   return last_error();
 }
