@@ -294,7 +294,7 @@ class Engine:
             if download:
                 for x, _ in results:
                     x.to_numpy()
-            return results, [ms] * len(results)
+            return results, handle.latencies_ms()
         lat = []
         results = []
         if self.kind == "plain":
@@ -479,7 +479,7 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
             step_ms.append(ms)
             res = batch.collect()
             ok += sum(1 for r in res if r.status == 0 and r.info.converged)
-            lats.extend([ms] * len(res))
+            lats.extend(batch.latencies_ms())
             flops += batch.gemm_flops()
     barrier()
     total_ms = sum(step_ms)

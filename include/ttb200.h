@@ -428,8 +428,12 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * of the block's dense products (2 m n k each; factorisations not
  * counted), residuals[2 * max_sweeps + 1] the operator applications and
  * residuals[2 * max_sweeps + 2 .. + 8] SM cycles spent in environment
- * updates, local solves, residual cores, truncation with enrichment, (unused),
- * residual checks and set-up; x core k at slab + x_offsets[k].  local_rtol > 0
+ * updates, local solves, residual cores, truncation with enrichment, dense
+ * products (a part of the other phases), residual checks and set-up,
+ * residuals[2 * max_sweeps + 10] and [+ 11] the device's global timer (ns)
+ * when the block started and finished the solve; x core k at
+ * slab + x_offsets[k].  Blocks start in task order, so listing the longest
+ * solves first shortens the launch.  local_rtol > 0
  * selects MINRES for local systems above direct_solve_size unknowns (at
  * most min(5 N, 2000) iterations per call, SciPy's cap being 5 N);
  * local_rtol <= 0 refuses them (status -5).

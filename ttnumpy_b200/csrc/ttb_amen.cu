@@ -57,8 +57,17 @@ struct Ctx {
   long long cyc[8];       // SM cycles per phase (see PH_*)
 };
 
-// phases timed with clock64 for the per-solve breakdown
-enum { PH_ENV = 0, PH_SOLVE, PH_ZCORE, PH_TRUNC, PH_ENRICH, PH_RESID, PH_INIT, PH_N };
+// the device-wide nanosecond timer (comparable across SMs)
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// phases timed with clock64 for the per-solve breakdown; PH_GEMM is not a
+// phase of its own: it sums the cycles of every dense product (inside the
+// other phases), to measure the block's GEMM rate
+enum { PH_ENV = 0, PH_SOLVE, PH_ZCORE, PH_TRUNC, PH_GEMM, PH_RESID, PH_INIT, PH_N };
 
 __device__ double* take(Ctx& c, i64 n) {
   n = (n + 31) & ~31LL;
@@ -98,11 +107,13 @@ __device__ double vnorm_diff(const double* x, const double* y, i64 n, double* re
   return sqrt(block_sum(s, red));
 }
 
-__device__ void gemm(Ctx& c, CMat A, CMat B, Mat C, int M, int N, int K, double alpha,
-                     double beta) {
+__device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, Mat C, int M, int N, int K,
+                                  double alpha, double beta) {
   if (M <= 0 || N <= 0) return;
   c.flops += 2.0 * M * N * (double)K;
+  const long long t0 = clock64();
   cta_gemm(A, B, C, M, N, K, alpha, beta, c.sm->gsm);
+  c.cyc[PH_GEMM] += clock64() - t0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1051,6 +1062,7 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
   c.applies = 0;
   c.check = 0.0;
   for (int i = 0; i < PH_N; ++i) c.cyc[i] = 0;
+  const unsigned long long t_start = global_ns();
   long long t_ph = clock64();
 #define PHASE(ph)                         \
   {                                       \
@@ -1283,6 +1295,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
     T->residuals[2 * T->max_sweeps + 1] = (double)c.applies;
     for (int i = 0; i < PH_N; ++i) T->residuals[2 * T->max_sweeps + 2 + i] = (double)c.cyc[i];
     T->residuals[2 * T->max_sweeps + 2 + PH_N] = c.check;
+    T->residuals[2 * T->max_sweeps + 10] = (double)t_start;
+    T->residuals[2 * T->max_sweeps + 11] = (double)global_ns();
   }
 #undef PHASE
 #undef CHECK

@@ -87,28 +87,42 @@ struct CMat {
 };
 
 // ---------------------------------------------------------------------------
-// GEMM: one 64x64 output tile per call, K staged through shared memory
+// GEMM: one 64x64 output tile per call, K staged through shared memory,
+// products on the FP64 tensor-core path (mma.sync m8n8k4 .f64)
 // ---------------------------------------------------------------------------
 
 constexpr int GBM = 64, GBN = 64, GBK = 16;
+// Row pitch of the staged tiles: 68 doubles puts the four k-rows a fragment
+// load touches on disjoint bank groups, so each load takes two wavefronts.
+constexpr int GPITCH = 68;
 
 struct GemmSmem {
-  double a[GBK][GBM + 1];
-  double b[GBK][GBN + 1];
+  double a[GBK][GPITCH];  // a[k][m]
+  double b[GBK][GPITCH];  // b[k][n]
 };
 
+// D += A(8x4, row) * B(4x8, col) in FP64; lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+static __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // C[m0:m0+64, n0:n0+64] = alpha * A * B + beta * C over the full K range.
-// A is M x K, B is K x N.  beta == 0 never reads C.  Thread (tx, ty) of a
-// 16 x 16 grid owns rows ty + 16 i and columns tx + 16 j.
+// A is M x K, B is K x N.  beta == 0 never reads C.  The eight warps form a
+// 2 x 4 grid of 32 x 16 warp tiles, each 4 x 2 MMA tiles of 8 x 8.
 static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0, int n0,
                               double alpha, double beta, GemmSmem& sm) {
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[4][2][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   // loads walk the unit-stride direction of each operand when there is one
   const bool a_kfast = (A.cs == 1);
@@ -146,38 +160,40 @@ static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K,
     __syncthreads();  // previous compute finished with the tile
     store();
     __syncthreads();
-    if (k0 + GBK < K) load(k0 + GBK);  // prefetch overlaps the FMAs below
+    if (k0 + GBK < K) load(k0 + GBK);  // prefetch overlaps the MMAs below
 #pragma unroll
-    for (int k = 0; k < GBK; ++k) {
-      double av[4], bv[4];
+    for (int kk = 0; kk < GBK; kk += 4) {
+      double av[4], bv[2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = sm.a[k][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) av[i] = sm.a[kk + t][wm + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = sm.b[k][tx + 16 * j];
+      for (int j = 0; j < 2; ++j) bv[j] = sm.b[kk + t][wn + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
     }
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    int gm = m0 + ty + 16 * i;
+    const int gm = m0 + wm + 8 * i + g;
     if (gm >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int gn = n0 + tx + 16 * j;
-      if (gn >= N) continue;
-      double v = alpha * acc[i][j];
-      if (beta != 0.0) v = fma(beta, C(gm, gn), v);
-      C(gm, gn) = v;
-    }
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gn = n0 + wn + 8 * j + 2 * t + h;
+        if (gn >= N) continue;
+        double v = alpha * acc[i][j][h];
+        if (beta != 0.0) v = fma(beta, C(gm, gn), v);
+        C(gm, gn) = v;
+      }
   }
   __syncthreads();  // callers may reuse the staging buffers right away
 }
 
 // Whole product, looping over all output tiles with the one block.
-static __device__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
+static __device__ __noinline__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
                          GemmSmem& sm) {
   for (int m0 = 0; m0 < M; m0 += GBM)
     for (int n0 = 0; n0 < N; n0 += GBN) cta_gemm_tile(A, B, C, M, N, K, m0, n0, alpha, beta, sm);

@@ -173,9 +173,12 @@ class PersistentBatch:
         self.xoff = torch.zeros(n, self.dmax, dtype=torch.int64, device="cuda")
         tasks = (Task * n)()
         base_in, base_off = self.dev_in.data_ptr(), self.dev_off.data_ptr()
+        # blocks start in task order: longest solves first (estimated cost)
+        self.order = sorted(range(n), key=lambda i: -_cost(preps[i]))
+        slot = {i: j for j, i in enumerate(self.order)}
         opos = 0
         for i, p in enumerate(preps):
-            t = tasks[i]
+            t = tasks[slot[i]]
             ptrs = []
             for _ in range(4):
                 ptrs.append(base_off + 8 * opos)
@@ -223,22 +226,35 @@ class PersistentBatch:
         resid_h = self.resid.cpu().numpy()
         return float(sum(resid_h[i, 2 * p.st.max_sweeps] for i, p in enumerate(self.preps)))
 
-    PHASES = ("env", "solve", "zcore", "trunc_enrich", "enrich", "resid", "init")
+    PHASES = ("env", "solve", "zcore", "trunc_enrich", "gemm", "resid", "init")
 
     def breakdown(self):
         """Per solve: operator applications and SM cycles per phase of the
         last launch (environment updates, local solves, residual cores,
-        truncation with enrichment, residual checks, set-up)."""
+        truncation with enrichment, residual checks, set-up) and, under
+        "gemm", the cycles of all dense products (inside those phases)."""
         resid_h = self.resid.cpu().numpy()
         out = []
         for i, p in enumerate(self.preps):
             base = 2 * p.st.max_sweeps
-            row = {"applies": int(resid_h[i, base + 1])}
+            row = {"applies": int(resid_h[i, base + 1]), "flops": float(resid_h[i, base])}
             for j, name in enumerate(self.PHASES):
                 row[name] = float(resid_h[i, base + 2 + j])
             row["check"] = float(resid_h[i, base + 9])
             out.append(row)
         return out
+
+    def latencies_ms(self) -> List[float]:
+        """Per solve of the last launch: milliseconds from the first block's
+        start to this solve's end (device global timer)."""
+        resid_h = self.resid.cpu().numpy()
+        starts, ends = [], []
+        for i, p in enumerate(self.preps):
+            base = 2 * p.st.max_sweeps
+            starts.append(resid_h[i, base + 10])
+            ends.append(resid_h[i, base + 11])
+        t0 = min(starts)
+        return [(e - t0) * 1e-6 for e in ends]
 
     def collect(self) -> List[Result]:
         """Results of the last launch (synchronises with it)."""
@@ -276,6 +292,14 @@ class PersistentBatch:
     def run(self, stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
         self.launch(stream)
         return self.collect()
+
+
+def _cost(p: "_Prepared") -> float:
+    """Relative cost estimate of a solve for the launch order: the local
+    apply grows like n^3 R^2 at the bonds such problems reach, times d."""
+    n = max(p.modes)
+    R = max(c.shape[0] for c in p.A)
+    return float(p.d) * n ** 3 * R ** 2
 
 
 def prepare(requests: Sequence) -> List["_Prepared"]:
