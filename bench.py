@@ -39,7 +39,7 @@ import numpy as np  # noqa: E402
 METRIC = "AMEn solves/s at relative residual 1e-8"
 UNIT = "solves/s"
 TOL = 1e-8
-MAX_SWEEPS = 20
+MAX_SWEEPS = 30
 
 
 def parse():
@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="requests in the CPU baseline sample (0: automatic)")
+    ap.add_argument("--diffusion-dims", default="4,5",
+                    help="dimensions d the diffusion requests draw from")
+    ap.add_argument("--diffusion-modes", default="16,32",
+                    help="mode sizes n the diffusion requests draw from")
     return ap.parse_args()
 
 
@@ -61,13 +65,14 @@ def parse():
 # ---------------------------------------------------------------------------
 
 
-def make_requests(count: int, seed: int):
+def make_requests(count: int, seed: int, dims=(4, 5), modes=(16, 32)):
     """Seeded request mix: half 2-D QTT Poisson (N ~ U{3..10}, sin*sin
-    right-hand side), half parametric diffusion (d ~ U{4,5}, n ~ U{16,32},
+    right-hand side), half parametric diffusion (d ~ U(dims), n ~ U(modes),
     theta ~ U(-1, 1))."""
     from ttnumpy_b200 import problems as P
 
     rng = np.random.default_rng(seed)
+    dims, modes = tuple(dims), tuple(modes)
     reqs = []
     for i in range(count):
         if i % 2 == 0:
@@ -75,12 +80,16 @@ def make_requests(count: int, seed: int):
             p = P.qtt_poisson_2d(N)
             p.meta["kind"] = "qtt"
         else:
-            d = int(rng.integers(4, 6))
-            n = int(rng.choice((16, 32)))
+            d = int(dims[int(rng.integers(0, len(dims)))])
+            n = int(rng.choice(modes))
             p = P.parametric_diffusion(d, n, rng.uniform(-1.0, 1.0, size=d))
             p.meta["kind"] = "diffusion"
         reqs.append(p)
     return reqs
+
+
+def _ints(text):
+    return [int(v) for v in str(text).split(",") if v.strip()]
 
 
 def solve_kwargs(p):
@@ -325,7 +334,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    reqs = make_requests(args.requests, args.seed)
+    reqs = make_requests(args.requests, args.seed, _ints(args.diffusion_dims),
+                         _ints(args.diffusion_modes))
     cores = cpu_cores()
     n_sample = args.cpu_sample or min(len(reqs), max(2 * cores, 8))
 
@@ -596,7 +606,8 @@ def config(args, reqs, engine="reference"):
     for p in reqs:
         kinds[p.meta["kind"]] = kinds.get(p.meta["kind"], 0) + 1
     return {"workload": "AMEn request mix: 2-D QTT Poisson (6-20 cores, mode 2) and parametric "
-                        "diffusion (d 4-5, mode 16/32), residual 1e-8",
+                        f"diffusion (d in {args.diffusion_dims}, mode in {args.diffusion_modes}), "
+                        "residual 1e-8",
             "requests_per_step": len(reqs), "mix": kinds, "engine": engine,
             "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
             "l2": "flushed (512 MB write) before every timed step",

@@ -107,7 +107,7 @@ __device__ double vnorm_diff(const double* x, const double* y, i64 n, double* re
   return sqrt(block_sum(s, red));
 }
 
-__device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, Mat C, int M, int N, int K,
+__device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, OMat C, int M, int N, int K,
                                   double alpha, double beta) {
   if (M <= 0 || N <= 0) return;
   c.flops += 2.0 * M * N * (double)K;
@@ -129,22 +129,24 @@ __device__ __noinline__ void env_step(Ctx& c, int side, const double* env, int t
       double* S1 = take(c, (i64)t * R * n * f2);
       double* S2 = take(c, (i64)t * m * R2 * f2);
       if (c.status) return;
-      gemm(c, CMat{env, f, 1}, CMat{frame, (i64)n * f2, 1}, Mat{S1, (i64)n * f2, 1}, t * R,
-           n * f2, f, 1.0, 0.0);
-      for (int tt = 0; tt < t; ++tt)
-        gemm(c, CMat{op, 1, (i64)m * R2}, CMat{S1 + (i64)tt * R * n * f2, f2, 1},
-             Mat{S2 + (i64)tt * m * R2 * f2, f2, 1}, m * R2, f2, R * n, 1.0, 0.0);
+      // S1[a, k, i, q] = sum_p env[i, a, p] frame[p, k, q]
+      gemm(c, CMat{env, f, 1}, CMat{frame, (i64)n * f2, 1},
+           OMat(S1, R, f2, (i64)n * t * f2, f2, (i64)t * f2, 1), t * R, n * f2, f, 1.0, 0.0);
+      // S2[i, l, b, q] = sum_{a, k} op[a, k, l, b] S1[(a, k), (i, q)]
+      gemm(c, CMat{op, 1, (i64)m * R2}, CMat{S1, (i64)t * f2, 1},
+           OMat(S2, kNoSplit, 0, f2, f2, (i64)m * R2 * f2, 1), m * R2, t * f2, R * n, 1.0, 0.0);
       gemm(c, CMat{target, 1, t2}, CMat{S2, (i64)R2 * f2, 1}, Mat{out, (i64)R2 * f2, 1}, t2,
            R2 * f2, t * m, 1.0, 0.0);
     } else {
       double* S1 = take(c, (i64)t2 * m * R * f);
       double* S2 = take(c, (i64)t2 * R2 * n * f);
       if (c.status) return;
-      gemm(c, CMat{target, t, 1}, CMat{env, (i64)R * f, 1}, Mat{S1, (i64)R * f, 1}, t2 * m,
-           R * f, t, 1.0, 0.0);
-      for (int tt = 0; tt < t2; ++tt)
-        gemm(c, CMat{op, (i64)m * R, 1}, CMat{S1 + (i64)tt * m * R * f, f, 1},
-             Mat{S2 + (i64)tt * R2 * n * f, f, 1}, R2 * n, f, m * R, 1.0, 0.0);
+      // S1[l, a, j, p] = sum_i target[j, l, i] env[i, a, p]
+      gemm(c, CMat{target, t, 1}, CMat{env, (i64)R * f, 1},
+           OMat(S1, m, f, (i64)R * t2 * f, f, (i64)t2 * f, 1), t2 * m, R * f, t, 1.0, 0.0);
+      // S2[j, b, k, p] = sum_{l, a} op[b, k, l, a] S1[(l, a), (j, p)]
+      gemm(c, CMat{op, (i64)m * R, 1}, CMat{S1, (i64)t2 * f, 1},
+           OMat(S2, kNoSplit, 0, f, f, (i64)R2 * n * f, 1), R2 * n, t2 * f, m * R, 1.0, 0.0);
       gemm(c, CMat{S2, (i64)n * f, 1}, CMat{frame, 1, (i64)n * f}, Mat{out, f2, 1}, t2 * R2, f2,
            n * f, 1.0, 0.0);
     }
@@ -225,6 +227,8 @@ struct LocalOp {
   const double* left;
   const double* op;
   const double* right;
+  const double* opP;     // op re-laid out as [a, l, k, b] (permute_op)
+  const double* rightP;  // right re-laid out as [b, p, q] (permute_op)
   int lt, lf, R, R2, n, m, rt, rf;
 };
 
@@ -239,26 +243,64 @@ __device__ LocalOp local_A(Ctx& c, int k) {
   L.R = s->R[k];
   L.R2 = s->R[k + 1];
   L.n = L.m = s->n[k];
+  L.opP = L.rightP = nullptr;
   return L;
 }
 
-// y = alpha * B x + beta * y for ``cols`` vectors (ttb_local_apply's chain)
+// The operator core and the right environment re-laid out (on the stack,
+// released with the caller's mark) so that every product of apply() and of
+// the forward rank-one terms is one GEMM over plain strides:
+// opP[a, l, k, b] = op[a, k, l, b] and rightP[b, p, q] = right[p, b, q].
+__device__ __noinline__ void permute_op(Ctx& c, LocalOp& L) {
+  const int R = L.R, R2 = L.R2, n = L.n, m = L.m, rt = L.rt, rf = L.rf;
+  const i64 no = (i64)R * m * n * R2, nr = (i64)R2 * rt * rf;
+  double* opP = take(c, no);
+  double* rightP = take(c, nr);
+  if (c.status) return;
+  for (i64 e = threadIdx.x; e < no; e += TTB_THREADS) {
+    const int b = (int)(e % R2);
+    const int k = (int)((e / R2) % n);
+    const int l = (int)((e / ((i64)R2 * n)) % m);
+    const int a = (int)(e / ((i64)R2 * n * m));
+    opP[e] = L.op[(((i64)a * n + k) * m + l) * R2 + b];
+  }
+  for (i64 e = threadIdx.x; e < nr; e += TTB_THREADS) {
+    const int q = (int)(e % rf);
+    const int pp = (int)((e / rf) % rt);
+    const int b = (int)(e / ((i64)rf * rt));
+    rightP[e] = L.right[((i64)pp * R2 + b) * rf + q];
+  }
+  __syncthreads();
+  L.opP = opP;
+  L.rightP = rightP;
+}
+
+// y = alpha * B x + beta * y for ``cols`` vectors (one_site.py:78-115) as
+// three GEMMs per vector, contracting the left bond, then the operator's
+// (bond, mode) pair, then the right bond; the first two write their results
+// permuted (split-index outputs) so that each next product reads plain
+// strides.  Needs permute_op(L).
 __device__ __noinline__ void apply(Ctx& c, const LocalOp& L, const double* x, double* y, int cols,
                       double alpha, double beta) {
+  const int lt = L.lt, lf = L.lf, R = L.R, R2 = L.R2, n = L.n, m = L.m, rt = L.rt, rf = L.rf;
   const i64 mark = c.top;
   c.applies += cols;
-  double* T1 = take(c, (i64)cols * L.lt * L.m * L.R2 * L.rf);
-  double* T2 = take(c, (i64)cols * L.lt * L.R * L.n * L.rf);
+  double* W1 = take(c, (i64)R * m * lf * rt);   // W1[a, l, j, p]
+  double* W2 = take(c, (i64)lf * n * R2 * rt);  // W2[j, k, b, p]
   if (c.status) return;
-  gemm(c, CMat{x, L.rt, 1}, CMat{L.right, (i64)L.R2 * L.rf, 1}, Mat{T1, (i64)L.R2 * L.rf, 1},
-       cols * L.lt * L.m, L.R2 * L.rf, L.rt, 1.0, 0.0);
-  for (int ci = 0; ci < cols * L.lt; ++ci)
-    gemm(c, CMat{L.op, (i64)L.m * L.R2, 1}, CMat{T1 + (i64)ci * L.m * L.R2 * L.rf, L.rf, 1},
-         Mat{T2 + (i64)ci * L.R * L.n * L.rf, L.rf, 1}, L.R * L.n, L.rf, L.m * L.R2, 1.0, 0.0);
-  for (int cc = 0; cc < cols; ++cc)
-    gemm(c, CMat{L.left, 1, L.lf}, CMat{T2 + (i64)cc * L.lt * L.R * L.n * L.rf, (i64)L.n * L.rf, 1},
-         Mat{y + (i64)cc * L.lf * L.n * L.rf, (i64)L.n * L.rf, 1}, L.lf, L.n * L.rf, L.lt * L.R,
-         alpha, beta);
+  for (int cc = 0; cc < cols; ++cc) {
+    const double* xc = x + (i64)cc * lt * m * rt;
+    double* yc = y + (i64)cc * lf * n * rf;
+    // W1[(a, j), (l, p)] = sum_i left[i, a, j] x[i, l, p]
+    gemm(c, CMat{L.left, 1, (i64)R * lf}, CMat{xc, (i64)m * rt, 1},
+         OMat(W1, lf, (i64)m * lf * rt, rt, rt, (i64)lf * rt, 1), R * lf, m * rt, lt, 1.0, 0.0);
+    // W2[(k, b), (j, p)] = sum_{a, l} op[a, k, l, b] W1[(a, l), (j, p)]
+    gemm(c, CMat{L.opP, 1, (i64)n * R2}, CMat{W1, (i64)lf * rt, 1},
+         OMat(W2, kNoSplit, 0, rt, rt, (i64)n * R2 * rt, 1), n * R2, lf * rt, R * m, 1.0, 0.0);
+    // y[(j, k), q] = alpha * sum_{b, p} W2[(j, k), (b, p)] right[p, b, q] + beta * y
+    gemm(c, CMat{W2, (i64)R2 * rt, 1}, CMat{L.rightP, rf, 1}, Mat{yc, rf, 1}, lf * n, rf,
+         R2 * rt, alpha, beta);
+  }
   c.top = mark;
 }
 
@@ -516,9 +558,10 @@ __device__ __noinline__ void solve_local(Ctx& c, int k, const double* b_loc, dou
     c.status = ST_SETTINGS;
     return;
   }
+  const i64 mark = c.top;
+  permute_op(c, L);
   vcopy(u, xcore(c, k), N);  // warm start: the current centre core
   __syncthreads();
-  const i64 mark = c.top;
   double* tmp = take(c, N);
   if (c.status) return;
   const double bn = vnorm_diff(b_loc, nullptr, N, c.sm->red);
@@ -563,18 +606,16 @@ __device__ __noinline__ void rank1_apply(Ctx& c, const LocalOp& L, bool forward,
   const i64 mark = c.top;
   if (forward) {
     // u_r[i, l] = s_r U[(i, l), r]; v_r[p'] = Vh[r, p']
-    double* P = take(c, (i64)R * lf * m);
+    double* P = take(c, (i64)lf * R * m);  // P[j, a, l]
     double* Y = take(c, (i64)lf * n * R2);
     double* W = take(c, (i64)R2 * rf);
     if (c.status) return;
-    for (int a = 0; a < R; ++a)
-      gemm(c, CMat{L.left + (i64)a * lf, 1, (i64)R * lf}, CMat{U + r, (i64)m * p, p},
-           Mat{P + (i64)a * lf * m, m, 1}, lf, m, lt, sr, 0.0);
-    for (int a = 0; a < R; ++a)
-      for (int b = 0; b < R2; ++b)
-        gemm(c, CMat{P + (i64)a * lf * m, m, 1},
-             CMat{L.op + (i64)a * n * m * R2 + b, R2, (i64)m * R2},
-             Mat{Y + b, (i64)n * R2, R2}, lf, n, m, 1.0, a == 0 ? 0.0 : 1.0);
+    // P[j, (a, l)] = s_r sum_i left[i, a, j] U[(i, l), r]
+    gemm(c, CMat{L.left, 1, (i64)R * lf}, CMat{U + r, (i64)m * p, p},
+         OMat(P, lf, m, (i64)R * m, kNoSplit, 0, 1), R * lf, m, lt, sr, 0.0);
+    // Y[j, (k, b)] = sum_{a, l} P[j, (a, l)] op[a, k, l, b]
+    gemm(c, CMat{P, (i64)R * m, 1}, CMat{L.opP, (i64)n * R2, 1}, Mat{Y, (i64)n * R2, 1}, lf,
+         n * R2, R * m, 1.0, 0.0);
     gemm(c, CMat{Vh + (i64)r * rt, 0, 1}, CMat{L.right, (i64)R2 * rf, 1}, Mat{W, 0, 1}, 1,
          R2 * rf, rt, 1.0, 0.0);
     gemm(c, CMat{Y, R2, 1}, CMat{W, rf, 1}, Mat{out, rf, 1}, lf * n, rf, R2, 1.0, 0.0);
@@ -588,11 +629,9 @@ __device__ __noinline__ void rank1_apply(Ctx& c, const LocalOp& L, bool forward,
          0.0);
     gemm(c, CMat{Vh + (i64)r * m * rt, rt, 1}, CMat{L.right, (i64)R2 * rf, 1},
          Mat{Q, (i64)R2 * rf, 1}, m, R2 * rf, rt, 1.0, 0.0);
-    for (int a = 0; a < R; ++a)
-      for (int b = 0; b < R2; ++b)
-        gemm(c, CMat{L.op + (i64)a * n * m * R2 + b, (i64)m * R2, R2},
-             CMat{Q + (i64)b * rf, (i64)R2 * rf, 1}, Mat{Z + (i64)a * n * rf, rf, 1}, n, rf, m,
-             1.0, b == 0 ? 0.0 : 1.0);
+    // Z[(a, k), q] = sum_{l, b} op[(a, k), (l, b)] Q[(l, b), q]
+    gemm(c, CMat{L.op, (i64)m * R2, 1}, CMat{Q, rf, 1}, Mat{Z, rf, 1}, R * n, rf, m * R2, 1.0,
+         0.0);
     gemm(c, CMat{yv, 1, lf}, CMat{Z, (i64)n * rf, 1}, Mat{out, (i64)n * rf, 1}, lf, n * rf, R,
          1.0, 0.0);
   }
@@ -619,6 +658,7 @@ __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const do
   LocalOp L = local_A(c, k);
   const i64 N = (i64)M * Kc;
   const i64 mark = c.top;
+  permute_op(c, L);
   double* tmp = take(c, N);
   double* part = take(c, N);
   double* term = take(c, N);
@@ -794,7 +834,10 @@ __device__ __noinline__ void residual_core(Ctx& c, int k, const double* u, doubl
   L.R = s->R[k];
   L.R2 = s->R[k + 1];
   L.n = L.m = n;
+  const i64 mark = c.top;
+  permute_op(c, L);
   apply(c, L, u, out, 1, -1.0, 1.0);
+  c.top = mark;
 }
 
 // forward step after the solve: truncate, enrich, shift x and z
@@ -1333,7 +1376,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   // the sub-steps, each term rounded up generously
   const long long r = rmax, n = nmax, R = Rmax, N = r * n * r, cols = r + K;
   const long long env = 2 * r * R * n * r + r * n * r;
-  const long long apply = 2 * r * n * R * r;
+  const long long apply = 2 * r * n * R * r + R * n * n * R + R * r * r;  // + permute_op
   const long long dn = std::min<long long>(direct_solve_size, N);
   const long long direct = dn * dn + dn;
   const long long iter = N + 7 * N + apply;

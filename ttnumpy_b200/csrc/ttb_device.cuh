@@ -109,11 +109,34 @@ static __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double
                : "d"(a), "d"(b));
 }
 
+// GEMM output view whose row and column indices may each be split in two:
+// (i, j) -> p + (i / rdiv) * rs_hi + (i % rdiv) * rs
+//             + (j / cdiv) * cs_hi + (j % cdiv) * cs.
+// A plain Mat converts to the unsplit form.  The split lets one product write
+// a result whose two index groups interleave in memory (a tensor
+// contraction's output permuted for the next contraction).
+constexpr int kNoSplit = 1 << 30;
+struct OMat {
+  double* p;
+  i64 rs, cs, rs_hi, cs_hi;
+  int rdiv, cdiv;
+  __device__ OMat(Mat m)
+      : p(m.p), rs(m.rs), cs(m.cs), rs_hi(0), cs_hi(0), rdiv(kNoSplit), cdiv(kNoSplit) {}
+  __device__ OMat(double* p_, int rdiv_, i64 rs_hi_, i64 rs_, int cdiv_, i64 cs_hi_, i64 cs_)
+      : p(p_), rs(rs_), cs(cs_), rs_hi(rs_hi_), cs_hi(cs_hi_), rdiv(rdiv_), cdiv(cdiv_) {}
+  __device__ __forceinline__ i64 row(int i) const {
+    return rdiv == kNoSplit ? i * rs : (i / rdiv) * rs_hi + (i % rdiv) * rs;
+  }
+  __device__ __forceinline__ i64 col(int j) const {
+    return cdiv == kNoSplit ? j * cs : (j / cdiv) * cs_hi + (j % cdiv) * cs;
+  }
+};
+
 // C[m0:m0+64, n0:n0+64] = alpha * A * B + beta * C over the full K range.
 // A is M x K, B is K x N.  beta == 0 never reads C.  The eight warps form a
 // 2 x 4 grid of 32 x 16 warp tiles, each 4 x 2 MMA tiles of 8 x 8.
-static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K, int m0, int n0,
-                              double alpha, double beta, GemmSmem& sm) {
+static __device__ void cta_gemm_tile(CMat A, CMat B, const OMat& C, int M, int N, int K, int m0,
+                                     int n0, double alpha, double beta, GemmSmem& sm) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
@@ -174,10 +197,16 @@ static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K,
         for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
     }
   }
+  i64 coff[2][2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) coff[j][h] = C.col(n0 + wn + 8 * j + 2 * t + h);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int gm = m0 + wm + 8 * i + g;
     if (gm >= M) continue;
+    double* crow = C.p + C.row(gm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -185,15 +214,15 @@ static __device__ void cta_gemm_tile(CMat A, CMat B, Mat C, int M, int N, int K,
         const int gn = n0 + wn + 8 * j + 2 * t + h;
         if (gn >= N) continue;
         double v = alpha * acc[i][j][h];
-        if (beta != 0.0) v = fma(beta, C(gm, gn), v);
-        C(gm, gn) = v;
+        if (beta != 0.0) v = fma(beta, crow[coff[j][h]], v);
+        crow[coff[j][h]] = v;
       }
   }
   __syncthreads();  // callers may reuse the staging buffers right away
 }
 
 // Whole product, looping over all output tiles with the one block.
-static __device__ __noinline__ void cta_gemm(CMat A, CMat B, Mat C, int M, int N, int K, double alpha, double beta,
+static __device__ __noinline__ void cta_gemm(CMat A, CMat B, OMat C, int M, int N, int K, double alpha, double beta,
                          GemmSmem& sm) {
   for (int m0 = 0; m0 < M; m0 += GBM)
     for (int n0 = 0; n0 < N; n0 += GBN) cta_gemm_tile(A, B, C, M, N, K, m0, n0, alpha, beta, sm);
