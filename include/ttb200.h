@@ -431,7 +431,8 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * updates, local solves, residual cores, truncation with enrichment, dense
  * products (a part of the other phases), residual checks and set-up,
  * residuals[2 * max_sweeps + 10] and [+ 11] the device's global timer (ns)
- * when the block started and finished the solve; x core k at
+ * when the block started and finished the solve (``residuals`` holds
+ * 2 * max_sweeps + 14 doubles); x core k at
  * slab + x_offsets[k].  Blocks start in task order, so listing the longest
  * solves first shortens the launch.  local_rtol > 0
  * selects MINRES for local systems above direct_solve_size unknowns (at
@@ -458,7 +459,10 @@ typedef struct {
   double residual_tol, error_threshold, residual_damp, stagnation_factor, local_rtol,
       truncation_tol;
   int debug; /* 1: also apply the operator to every rank-one term in full and
-                record the worst relative gap in residuals[2*max_sweeps + 9] */
+                record the worst relative gap in residuals[2*max_sweeps + 9];
+                repeat every two-level R-only QR with the one-level one and
+                record the worst relative gap of R in [2*max_sweeps + 12],
+                the number of such QRs in [+ 13] */
 } ttb_amen_task_t;
 long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int rmax,
                                 int direct_solve_size);

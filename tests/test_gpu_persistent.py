@@ -129,3 +129,20 @@ def test_rank1_factorisation_self_check(pers):
     checks = [row["check"] for row in batch.breakdown()]
     assert max(checks) < 1e-11, checks
     assert checks[0] > 0.0  # the diffusion solve truncated with residual-budget ranks
+
+
+def test_two_level_qr_self_check(pers):
+    """The residual-norm sweep factorises tall matrices (rows >= 4 x columns,
+    more than 64 columns) with the two-level blocked R-only QR; in debug mode
+    each such factorisation is repeated with the one-level blocked QR and the
+    worst relative gap of R is recorded (rounding only)."""
+    kw = dict(residual_tol=1e-8, symmetric=True, max_sweeps=6, seed=0, stagnation_factor=None)
+    reqs = [(p.A, p.b, None, kw) for p in (_diffusion(4, 4, 32), _diffusion(5, 5, 16))]
+    batch = pers.PersistentBatch(pers.prepare(reqs), 64, debug=True)
+    out = batch.run()
+    assert all(r.status == 0 for r in out)
+    rows = batch.breakdown()
+    assert sum(row["n_qr2"] for row in rows) > 0
+    # Householder QR is backward stable with ||dR|| <= c m eps ||A||; for
+    # m ~ 2000-7000 rows the two orders of summation differ by ~1e-12
+    assert max(row["check_qr"] for row in rows) < 1e-10, rows

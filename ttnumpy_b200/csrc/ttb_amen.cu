@@ -54,6 +54,8 @@ struct Ctx {
   double flops;  // FP64 FLOPs of the block's GEMMs (2 m n k each)
   long long applies;      // one-site operator applications
   double check;           // debug: worst relative gap of the factorised term products
+  double check_qr;        // debug: worst relative gap of the two-level R-only QR
+  int n_qr2;              // debug: two-level R-only QRs checked
   long long cyc[8];       // SM cycles per phase (see PH_*)
 };
 
@@ -331,6 +333,31 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   const i64 mark = c.top;
   double* W = take(c, (i64)m * k + p);
   if (c.status) return;
+  if (!Q.p && p > LNB2 && m >= 4 * k) {
+    // R only of a tall matrix (the residual norm sweep): two-level blocking
+    cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, c.sm->gsm);
+    if (c.T->debug) {
+      // the one-level blocked factorisation of the same matrix, compared
+      double* R1 = take(c, (i64)p * k);
+      if (c.status) return;
+      cta_qr_blocked(A, m, k, W, W + (i64)m * k, Mat{nullptr, 0, 0}, Mat{R1, k, 1}, c.pool,
+                     c.pool + (i64)LNB * YCH, c.pool + (i64)LNB * YCH + LNB * LNB, c.sm->red,
+                     c.sm->gsm);
+      double dsq = 0.0, rsq = 0.0;
+      for (i64 e = threadIdx.x; e < (i64)p * k; e += TTB_THREADS) {
+        const int i = (int)(e / k), j = (int)(e % k);
+        const double a = R(i, j), b = R1[e];
+        dsq = fma(a - b, a - b, dsq);
+        rsq = fma(b, b, rsq);
+      }
+      dsq = block_sum(dsq, c.sm->red);
+      rsq = block_sum(rsq, c.sm->red);
+      c.check_qr = fmax(c.check_qr, rsq > 0.0 ? sqrt(dsq / rsq) : sqrt(dsq));
+      c.n_qr2 += 1;
+    }
+    c.top = mark;
+    return;
+  }
   double* Y = c.pool;
   double* G = Y + (i64)LNB * YCH;
   double* Tm = G + LNB * LNB;
@@ -1104,6 +1131,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
   c.flops = 0.0;
   c.applies = 0;
   c.check = 0.0;
+  c.check_qr = 0.0;
+  c.n_qr2 = 0;
   for (int i = 0; i < PH_N; ++i) c.cyc[i] = 0;
   const unsigned long long t_start = global_ns();
   long long t_ph = clock64();
@@ -1338,6 +1367,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
     T->residuals[2 * T->max_sweeps + 1] = (double)c.applies;
     for (int i = 0; i < PH_N; ++i) T->residuals[2 * T->max_sweeps + 2 + i] = (double)c.cyc[i];
     T->residuals[2 * T->max_sweeps + 2 + PH_N] = c.check;
+    T->residuals[2 * T->max_sweeps + 12] = c.check_qr;
+    T->residuals[2 * T->max_sweeps + 13] = (double)c.n_qr2;
     T->residuals[2 * T->max_sweeps + 10] = (double)t_start;
     T->residuals[2 * T->max_sweeps + 11] = (double)global_ns();
   }

@@ -762,6 +762,110 @@ static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* t
   __syncthreads();
 }
 
+// R factor only of the economic QR of the m x k view A, two-level blocked
+// for tall operands: outer panels of LNB2 columns are factorised by the
+// LNB-blocked Householder code (trailing updates inside the panel only),
+// then the panel's LNB2 reflectors update the rest of the matrix as one
+// compact-WY block, C -= V (T^T (V^T C)), whose products have 64-wide tiles
+// and long K.  Same reflectors as cta_qr_blocked.  W (m x k column major)
+// and tau (min(m, k)) are global work; ``pool`` (shared) holds
+// 2 LNB2^2 + LNB2^2 + LNB * LNB2 + 2 LNB^2 doubles.
+constexpr int LNB2 = 64;
+static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, double* W, double* tau,
+                                                      Mat R, double* pool, double* red,
+                                                      GemmSmem& gsm) {
+  const int p = m < k ? m : k;
+  const int tid = threadIdx.x;
+  double* G2 = pool;                      // LNB2 x LNB2: V^T V, later T^T Y
+  double* T2 = G2 + LNB2 * LNB2;          // LNB2 x LNB2 upper triangular
+  double* Yo = T2 + LNB2 * LNB2;          // LNB2 x LNB2 chunk of V^T C
+  double* Yi = Yo + LNB2 * LNB2;          // LNB x LNB2 (inner updates)
+  double* Gi = Yi + LNB * LNB2;
+  double* Ti = Gi + LNB * LNB;
+  cta_copy(A, Mat{W, 1, (i64)m}, m, k);
+  __syncthreads();
+  for (int o0 = 0; o0 < p; o0 += LNB2) {
+    const int ob = min(LNB2, p - o0);
+    const int orows = m - o0;
+    double* Wo = W + o0 + (i64)o0 * m;
+    // inner LNB-blocked factorisation of the panel's ob columns
+    for (int j0 = o0; j0 < o0 + ob; j0 += LNB) {
+      const int jb = min(LNB, o0 + ob - j0);
+      const int rows = m - j0;
+      double* Wp = W + j0 + (i64)j0 * m;
+      cta_householder(Wp, rows, jb, m, tau + j0, red);
+      for (int e = tid; e < jb * jb; e += TTB_THREADS) {
+        int r = e % jb, c = e / jb;
+        if (r <= c) {
+          R(j0 + r, j0 + c) = Wp[r + (i64)c * m];
+          Wp[r + (i64)c * m] = (r == c) ? 1.0 : 0.0;
+        }
+      }
+      __syncthreads();
+      const int nt = o0 + ob - j0 - jb;
+      if (nt > 0) {
+        cta_block_t(Wp, m, rows, jb, tau + j0, Gi, Ti, gsm);
+        double* C = W + j0 + (i64)(j0 + jb) * m;
+        cta_gemm(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Yi, 1, LNB}, jb, nt, rows, 1.0, 0.0, gsm);
+        for (int col = tid; col < nt; col += TTB_THREADS) {
+          double y[LNB];
+          for (int i = 0; i < jb; ++i) y[i] = Yi[i + (i64)col * LNB];
+          for (int i = jb - 1; i >= 0; --i) {
+            double acc = 0.0;
+            for (int q = 0; q <= i; ++q) acc = fma(Ti[q + i * LNB], y[q], acc);
+            Yi[i + (i64)col * LNB] = acc;
+          }
+        }
+        __syncthreads();
+        cta_gemm(CMat{Wp, 1, m}, CMat{Yi, 1, LNB}, Mat{C, 1, m}, rows, nt, jb, -1.0, 1.0, gsm);
+      }
+    }
+    // R entries above the inner diagonal blocks move out; V gets zeros there
+    for (int e = tid; e < ob * ob; e += TTB_THREADS) {
+      int r = e % ob, c = e / ob;
+      if (r < c && (r / LNB) != (c / LNB)) {
+        R(o0 + r, o0 + c) = Wo[r + (i64)c * m];
+        Wo[r + (i64)c * m] = 0.0;
+      }
+    }
+    __syncthreads();
+    const int nt = k - o0 - ob;
+    if (nt <= 0) continue;
+    // T of the panel: T[i, i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^T V)[0:i, i]
+    cta_gemm(CMat{Wo, m, 1}, CMat{Wo, 1, m}, Mat{G2, 1, LNB2}, ob, ob, orows, 1.0, 0.0, gsm);
+    for (int e = tid; e < LNB2 * LNB2; e += TTB_THREADS) T2[e] = 0.0;
+    __syncthreads();
+    for (int i = 0; i < ob; ++i) {
+      const double ti = tau[o0 + i];
+      for (int q = tid; q < i; q += TTB_THREADS) {
+        double acc = 0.0;
+        for (int r = q; r < i; ++r) acc = fma(T2[q + r * LNB2], G2[r + i * LNB2], acc);
+        T2[q + i * LNB2] = -ti * acc;
+      }
+      if (tid == 0) T2[i + i * LNB2] = ti;
+      __syncthreads();
+    }
+    for (int c0 = 0; c0 < nt; c0 += LNB2) {
+      const int nc = min(LNB2, nt - c0);
+      double* C = W + o0 + (i64)(o0 + ob + c0) * m;
+      // Yo = V^T C, G2 = T^T Yo, C -= V G2
+      cta_gemm(CMat{Wo, m, 1}, CMat{C, 1, m}, Mat{Yo, 1, LNB2}, ob, nc, orows, 1.0, 0.0, gsm);
+      cta_gemm(CMat{T2, LNB2, 1}, CMat{Yo, 1, LNB2}, Mat{G2, 1, LNB2}, ob, nc, ob, 1.0, 0.0, gsm);
+      cta_gemm(CMat{Wo, 1, m}, CMat{G2, 1, LNB2}, Mat{C, 1, m}, orows, nc, ob, -1.0, 1.0, gsm);
+    }
+  }
+  // the rest of R: below the diagonal zero, right of each outer panel from W
+  for (int e = tid; e < p * k; e += TTB_THREADS) {
+    int i = e % p, j = e / p;
+    if (i > j) {
+      R(i, j) = 0.0;
+    } else if (j >= min((i / LNB2) * LNB2 + LNB2, p)) {
+      R(i, j) = W[i + (i64)j * m];
+    }
+  }
+  __syncthreads();
+}
+
 // cta_svd_tall for matrices that do not fit in shared memory: blocked QR
 // into the global work area W, Jacobi on R in Bsq/V (global or shared), U
 // by the blocked reflector product.  Y needs LNB * max(k, 1) doubles, G and

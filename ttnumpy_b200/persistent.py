@@ -168,7 +168,7 @@ class PersistentBatch:
         self.slabs = torch.empty(int(self.slab_pos[-1]), dtype=torch.float64, device="cuda")
         self.dmax = max(p.d for p in preps)
         smax = max(max(p.st.max_sweeps for p in preps), 1)
-        self.resid = torch.zeros(n, 2 * smax + 12, dtype=torch.float64, device="cuda")
+        self.resid = torch.zeros(n, 2 * smax + 14, dtype=torch.float64, device="cuda")
         self.result = torch.zeros(n, 6 + self.dmax, dtype=torch.int32, device="cuda")
         self.xoff = torch.zeros(n, self.dmax, dtype=torch.int64, device="cuda")
         tasks = (Task * n)()
@@ -241,6 +241,8 @@ class PersistentBatch:
             for j, name in enumerate(self.PHASES):
                 row[name] = float(resid_h[i, base + 2 + j])
             row["check"] = float(resid_h[i, base + 9])
+            row["check_qr"] = float(resid_h[i, base + 12])
+            row["n_qr2"] = int(resid_h[i, base + 13])
             out.append(row)
         return out
 
