@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="persistent", choices=["plain", "served", "persistent"])
-    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--requests", type=int, default=592,
+                    help="requests per step (592 = 4 per SM of a B200)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="requests in the CPU baseline sample (0: automatic)")
@@ -86,6 +87,17 @@ def make_requests(count: int, seed: int, dims=(4, 5), modes=(16, 32)):
             p.meta["kind"] = "diffusion"
         reqs.append(p)
     return reqs
+
+
+# DRAM bytes (read + write) of one k_amen launch of the default workload,
+# from an ncu capture of `python bench.py`; other workloads report null
+DEFAULT_TRAFFIC = 655255445760 + 720370022144
+
+
+def _traffic(args):
+    default = (args.requests == 592 and args.seed == 0 and _ints(args.diffusion_dims) == [4, 5]
+               and _ints(args.diffusion_modes) == [16, 32])
+    return DEFAULT_TRAFFIC if default else None
 
 
 def _ints(text):
@@ -508,7 +520,9 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
     roof = {"kernel": "k_amen (ttb_amen_persistent)", "bound": "tensor", "unit": "TFLOP/s",
             "achieved": ach, "peak": fp64, "peak_source": "measured FP64 FMA probe "
             "(ttb_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
-            "frac": ach / fp64, "traffic": None,
+            "frac": ach / fp64, "traffic": _traffic(args),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                              "this workload (profiles/k_amen_bench_592req.md)",
             "flops_counted": "2mnk of every dense product the blocks ran; QR/SVD/LU not counted",
             "per_launch_us": 1e3 * sum(step_ms) / len(step_ms), "launches": len(step_ms)}
     cpu = None
