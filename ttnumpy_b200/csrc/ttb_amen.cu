@@ -21,7 +21,8 @@ namespace {
 using namespace ttb;
 
 constexpr int kD = 64;                 // most cores per train
-constexpr int kPoolBytes = 190 * 1024;  // dynamic shared-memory pool
+constexpr int kPoolBytes = 160 * 1024;  // dynamic shared-memory pool (after the GEMM ring)
+constexpr int kRingBytes = GSTAGES * GSTAGE_D * 8;
 constexpr i64 kPoolD = kPoolBytes / 8;
 constexpr int kMaxRestarts = 4;        // common.py:230
 constexpr double kShrink = 1e-2;       // common.py:233
@@ -40,7 +41,6 @@ struct Sm {
   int ipiv[LNB];
   int flag;
   i64 stack0;
-  GemmSmem gsm;
 };
 
 struct Ctx {
@@ -49,6 +49,8 @@ struct Ctx {
   double* slab;
   i64 cap, top;
   double* pool;
+  double* ring;   // shared staging ring of the pipelined GEMM
+  GemmSmem* gsm;  // its first stage, for the one-stage GEMM of the factorisations
   int d, rmax, K;
   int status;
   double flops;  // FP64 FLOPs of the block's GEMMs (2 m n k each)
@@ -114,7 +116,7 @@ __device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, OMat C, int M, int N, 
   if (M <= 0 || N <= 0) return;
   c.flops += 2.0 * M * N * (double)K;
   const long long t0 = clock64();
-  cta_gemm(A, B, C, M, N, K, alpha, beta, c.sm->gsm);
+  cta_gemm_pipe(A, B, C, M, N, K, alpha, beta, c.ring);
   c.cyc[PH_GEMM] += clock64() - t0;
 }
 
@@ -335,14 +337,14 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   if (c.status) return;
   if (!Q.p && p > LNB2 && m >= 4 * k) {
     // R only of a tall matrix (the residual norm sweep): two-level blocking
-    cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, c.sm->gsm);
+    cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, *c.gsm);
     if (c.T->debug) {
       // the one-level blocked factorisation of the same matrix, compared
       double* R1 = take(c, (i64)p * k);
       if (c.status) return;
       cta_qr_blocked(A, m, k, W, W + (i64)m * k, Mat{nullptr, 0, 0}, Mat{R1, k, 1}, c.pool,
                      c.pool + (i64)LNB * YCH, c.pool + (i64)LNB * YCH + LNB * LNB, c.sm->red,
-                     c.sm->gsm);
+                     *c.gsm);
       double dsq = 0.0, rsq = 0.0;
       for (i64 e = threadIdx.x; e < (i64)p * k; e += TTB_THREADS) {
         const int i = (int)(e / k), j = (int)(e % k);
@@ -361,7 +363,7 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   double* Y = c.pool;
   double* G = Y + (i64)LNB * YCH;
   double* Tm = G + LNB * LNB;
-  cta_qr_blocked(A, m, k, W, W + (i64)m * k, Q, R, Y, G, Tm, c.sm->red, c.sm->gsm);
+  cta_qr_blocked(A, m, k, W, W + (i64)m * k, Q, R, Y, G, Tm, c.sm->red, *c.gsm);
   c.top = mark;
 }
 
@@ -396,7 +398,7 @@ __device__ __noinline__ void svd(Ctx& c, CMat A, int m, int k, Mat U, double* S,
     double* G = Y + (i64)LNB * YCH;
     double* Tm = G + LNB * LNB;
     cta_svd_tall_blocked(At, M, K, W, tau, Bsq, V, sv, order, flag, Ut, S, Vt, Y, G, Tm,
-                         c.sm->red, c.sm->gsm);
+                         c.sm->red, *c.gsm);
   }
   c.top = mark;
 }
@@ -449,7 +451,7 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
     __syncthreads();
     if (info == 0) vcopy(u, bb, N);
   } else {
-    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, s->gsm);
+    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, *c.gsm);
   }
   __syncthreads();
   if (info != 0) c.status = ST_SINGULAR;
@@ -1114,8 +1116,9 @@ __device__ __noinline__ double train_norm(Ctx& c, int which) {
 
 __global__ void __launch_bounds__(TTB_THREADS, 1)
     k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
-  extern __shared__ double pool[];
+  extern __shared__ double dyn[];
   __shared__ Sm sm;
+  double* pool = dyn + GSTAGES * GSTAGE_D;
   const ttb_amen_task_t* T = tasks + blockIdx.x;
   Ctx c;
   c.T = T;
@@ -1124,6 +1127,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
   c.cap = T->slab_doubles;
   c.top = 0;
   c.pool = pool;
+  c.ring = dyn;
+  c.gsm = reinterpret_cast<GemmSmem*>(dyn);
   c.d = T->d;
   c.rmax = rmax;
   c.K = T->kickrank;
@@ -1427,7 +1432,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
 int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream) {
   if (count <= 0) return 0;
   static int configured = 0;
-  const size_t smem = kPoolBytes;
+  const size_t smem = kRingBytes + kPoolBytes;
   if (!configured) {
     cudaFuncSetAttribute(k_amen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = 1;

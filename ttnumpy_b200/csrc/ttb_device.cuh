@@ -229,6 +229,132 @@ static __device__ __noinline__ void cta_gemm(CMat A, CMat B, OMat C, int M, int 
 }
 
 // ---------------------------------------------------------------------------
+// Pipelined GEMM: the same 64x64 tiles and MMA fragments as cta_gemm_tile,
+// with operands copied by cp.async into a ring of GSTAGES shared-memory
+// stages.  The (output tile, k-tile) steps of the whole product form one
+// sequence, so loads run GSTAGES - 1 steps ahead across tile boundaries and
+// a tile's first operands arrive while the previous tile is finishing.
+// ``ring`` holds GSTAGES * 2 * GBK * GPITCH doubles of shared memory; its
+// first stage has the layout of GemmSmem.
+// ---------------------------------------------------------------------------
+
+constexpr int GSTAGES = 3;
+constexpr int GSTAGE_D = 2 * GBK * GPITCH;
+
+static __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = ok ? 8 : 0;  // 0 bytes read: the destination is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(sz)
+               : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+static __device__ __forceinline__ void cp_async_wait_ahead() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(GSTAGES - 2) : "memory");
+}
+static __device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
+                                                  double alpha, double beta, double* ring) {
+  if (M <= 0 || N <= 0) return;
+  if (K <= 0) {  // C = beta * C: the one-stage tile handles it
+    cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
+    return;
+  }
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+  const int g = lane >> 2, t = lane & 3;
+  const int tn = (N + GBN - 1) / GBN;
+  const int nk = (K + GBK - 1) / GBK;
+  const int total = ((M + GBM - 1) / GBM) * tn * nk;
+  const bool a_kfast = (A.cs == 1);
+  const bool b_nfast = (B.cs == 1) || (B.rs != 1);
+  auto issue = [&](int step) {
+    if (step < total) {
+      const int tile = step / nk, kt = step % nk;
+      const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN, k0 = kt * GBK;
+      double* sa = ring + (step % GSTAGES) * GSTAGE_D;
+      double* sb = sa + GBK * GPITCH;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int idx = tid + e * TTB_THREADS;
+        int mm, kk;
+        if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
+        const int gm = m0 + mm, gk = k0 + kk;
+        const bool oka = gm < M && gk < K;
+        cp_async8(sa + kk * GPITCH + mm, oka ? A.p + gm * A.rs + gk * A.cs : A.p, oka);
+        int nn, kb;
+        if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
+        const int gn = n0 + nn, gk2 = k0 + kb;
+        const bool okb = gn < N && gk2 < K;
+        cp_async8(sb + kb * GPITCH + nn, okb ? B.p + gk2 * B.rs + gn * B.cs : B.p, okb);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int st = 0; st < GSTAGES - 1; ++st) issue(st);
+  double acc[4][2][2];
+  for (int step = 0; step < total; ++step) {
+    const int kt = step % nk;
+    if (kt == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    }
+    cp_async_wait_ahead();
+    __syncthreads();  // this step's operands landed; the previous step's reads are done
+    issue(step + GSTAGES - 1);
+    const double* sa = ring + (step % GSTAGES) * GSTAGE_D;
+    const double* sb = sa + GBK * GPITCH;
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 4) {
+      double av[4], bv[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * GPITCH + wm + 8 * i + g];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) bv[j] = sb[(kk + t) * GPITCH + wn + 8 * j + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+    }
+    if (kt == nk - 1) {
+      const int tile = step / nk;
+      const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN;
+      i64 coff[2][2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) coff[j][h] = C.col(n0 + wn + 8 * j + 2 * t + h);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + wm + 8 * i + g;
+        if (gm >= M) continue;
+        double* crow = C.p + C.row(gm);
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int gn = n0 + wn + 8 * j + 2 * t + h;
+            if (gn >= N) continue;
+            double v = alpha * acc[i][j][h];
+            if (beta != 0.0) v = fma(beta, crow[coff[j][h]], v);
+            crow[coff[j][h]] = v;
+          }
+      }
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();  // callers may reuse the ring and read C right away
+}
+
+// ---------------------------------------------------------------------------
 // copies
 // ---------------------------------------------------------------------------
 
