@@ -337,7 +337,7 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   if (c.status) return;
   if (!Q.p && p > LNB2 && m >= 4 * k) {
     // R only of a tall matrix (the residual norm sweep): two-level blocking
-    cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, *c.gsm);
+    cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, c.ring);
     if (c.T->debug) {
       // the one-level blocked factorisation of the same matrix, compared
       double* R1 = take(c, (i64)p * k);
@@ -424,20 +424,31 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
     W = take(c, N * N);
     if (c.status) return;
   }
-  for (i64 e = threadIdx.x; e < N * N; e += TTB_THREADS) {
-    i64 row = e % N, col = e / N;
-    int nf = (int)(row % L.rf), kr = (int)((row / L.rf) % L.n), j = (int)(row / ((i64)L.rf * L.n));
-    int mt = (int)(col % L.rt), l = (int)((col / L.rt) % L.m), i = (int)(col / ((i64)L.rt * L.m));
-    double acc = 0.0;
-    for (int a = 0; a < L.R; ++a) {
-      const double la = L.left[((i64)i * L.R + a) * L.lf + j];
-      if (la == 0.0) continue;
-      const double* op = L.op + (((i64)a * L.n + kr) * L.m + l) * L.R2;
-      double t = 0.0;
-      for (int bb = 0; bb < L.R2; ++bb) t = fma(op[bb], L.right[((i64)mt * L.R2 + bb) * L.rf + nf], t);
-      acc = fma(la, t, acc);
+  // explicit local matrix, column major: each thread owns rows (j, kr, nf)
+  // and walks the columns (i, l, mt) in order (no divisions per element)
+  const int Nn = (int)N;
+  for (int row = threadIdx.x; row < Nn; row += TTB_THREADS) {
+    const int nf = row % L.rf, kr = (row / L.rf) % L.n, j = row / (L.rf * L.n);
+    int mt = 0, l = 0, i = 0;
+    for (int col = 0; col < Nn; ++col) {
+      double acc = 0.0;
+      for (int a = 0; a < L.R; ++a) {
+        const double la = L.left[(i * L.R + a) * L.lf + j];
+        if (la == 0.0) continue;
+        const double* op = L.op + ((a * L.n + kr) * L.m + l) * L.R2;
+        double t = 0.0;
+        for (int bb = 0; bb < L.R2; ++bb) t = fma(op[bb], L.right[(mt * L.R2 + bb) * L.rf + nf], t);
+        acc = fma(la, t, acc);
+      }
+      W[row + (i64)col * Nn] = acc;
+      if (++mt == L.rt) {
+        mt = 0;
+        if (++l == L.m) {
+          l = 0;
+          ++i;
+        }
+      }
     }
-    W[e] = acc;
   }
   vcopy(u, b, N);
   __syncthreads();
@@ -1063,7 +1074,38 @@ __device__ __noinline__ double train_norm(Ctx& c, int which) {
     int rows, cols;
     const int n = s->n[i];
     const double* core;
-    if (which == 0) {
+    const double* m = nullptr;
+    if (which == 0 && carry) {
+      // core i of A x - b times the carry without forming the core: the
+      // A x block as (x then A) contractions, the b block as one product
+      const int x1 = s->xb[i], x2 = s->xb[i + 1], R1 = s->R[i], R2 = s->R[i + 1];
+      const int rb1 = s->rb[i], rb2 = s->rb[i + 1];
+      const int ra = R1 * x1, ra2 = R2 * x2;
+      const bool first = (i == 0);
+      rows = first ? 1 : ra + rb1;
+      cols = ra2 + rb2;
+      double* mm = take(c, (i64)rows * n * cp);
+      double* T = take(c, (i64)n * R2 * x1 * cp);  // T[l, b, xr, q]
+      if (c.status) return 0.0;
+      const double* xc = xcore(c, i);
+      // T[(xr, l), q] = sum_xc x[xr, l, xc] carry[(b, xc), q] for each b
+      for (int bb = 0; bb < R2; ++bb)
+        gemm(c, CMat{xc, x2, 1}, CMat{carry + (i64)bb * x2 * cp, cp, 1},
+             OMat(T + (i64)bb * x1 * cp, n, cp, (i64)R2 * x1 * cp, kNoSplit, 0, 1), x1 * n, cp,
+             x2, 1.0, 0.0);
+      // mm[(a, xr), j, q] = sum_{l, b} A[a, j, l, b] T[(l, b), (xr, q)]
+      gemm(c, CMat{acore(c, i), (i64)n * R2, 1}, CMat{T, (i64)x1 * cp, 1},
+           OMat(mm, n, (i64)x1 * n * cp, cp, cp, (i64)n * cp, 1), R1 * n, x1 * cp, n * R2, 1.0,
+           0.0);
+      // b rows (the first core: the same row, accumulated), sign as in
+      // residual_train_core
+      const int kb = c.T->b_orth_center >= 0 ? c.T->b_orth_center : 0;
+      gemm(c, CMat{bcore(c, i), rb2, 1}, CMat{carry + (i64)ra2 * cp, cp, 1},
+           Mat{mm + (first ? 0 : (i64)ra * n * cp), cp, 1}, rb1 * n, cp, rb2,
+           (i == kb) ? -1.0 : 1.0, first ? 1.0 : 0.0);
+      m = mm;
+      core = nullptr;
+    } else if (which == 0) {
       const int ra = s->R[i] * s->xb[i], ra2 = s->R[i + 1] * s->xb[i + 1];
       const int rr = (i == 0) ? 1 : ra + s->rb[i];
       const int cc = (i == d - 1) ? 1 : ra2 + s->rb[i + 1];
@@ -1076,14 +1118,16 @@ __device__ __noinline__ double train_norm(Ctx& c, int which) {
       cols = s->rb[i + 1];
       core = bcore(c, i);
     }
-    const double* m = core;
-    if (carry) {
+    if (m) {
+      // formed above
+    } else if (carry) {
       double* mm = take(c, (i64)rows * n * cp);
       if (c.status) return 0.0;
       gemm(c, CMat{core, cols, 1}, CMat{carry, cp, 1}, Mat{mm, cp, 1}, rows * n, cp, cols, 1.0,
            0.0);
       m = mm;
     } else {
+      m = core;
       cp = cols;
     }
     if (i == 0) {

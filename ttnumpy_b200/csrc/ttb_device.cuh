@@ -235,7 +235,8 @@ static __device__ __noinline__ void cta_gemm(CMat A, CMat B, OMat C, int M, int 
 // sequence, so loads run GSTAGES - 1 steps ahead across tile boundaries and
 // a tile's first operands arrive while the previous tile is finishing.
 // ``ring`` holds GSTAGES * 2 * GBK * GPITCH doubles of shared memory; its
-// first stage has the layout of GemmSmem.
+// first stage has the layout of GemmSmem.  A and B may be anywhere (shared
+// operands take the one-stage path); C must not overlap the ring.
 // ---------------------------------------------------------------------------
 
 constexpr int GSTAGES = 3;
@@ -260,7 +261,9 @@ static __device__ __forceinline__ void cp_async_wait_all() {
 static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
                                                   double alpha, double beta, double* ring) {
   if (M <= 0 || N <= 0) return;
-  if (K <= 0) {  // C = beta * C: the one-stage tile handles it
+  // cp.async copies from global memory only: operands in shared memory, and
+  // K == 0 (C = beta * C), go through the one-stage tile
+  if (K <= 0 || __isShared(A.p) || __isShared(B.p)) {
     cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
     return;
   }
@@ -389,43 +392,82 @@ static __device__ __forceinline__ void cta_fill(Mat dst, int M, int N, double v)
 // tau = (beta - alpha) / beta, v = x / (alpha - beta); a column whose
 // sub-diagonal part is exactly zero gets tau = 0.
 static __device__ void cta_householder(double* W, int m, int k, i64 ldw, double* tau, double* red) {
+  // The whole block works on every reflector: the trailing columns are
+  // taken HC at a time, their dot products with v accumulated per thread
+  // over a row stripe and reduced together, and the squared norm of the
+  // next column is gathered during its update (one pass fewer per column).
+  constexpr int HC = 16;
+  __shared__ double hred[TTB_WARPS][HC];
+  __shared__ double hw[HC];
   const int p = m < k ? m : k;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double part = 0.0;
+  for (int i = 1 + tid; i < m; i += TTB_THREADS) part = fma(W[i], W[i], part);
+  double sigma = block_sum(part, red);
   for (int j = 0; j < p; ++j) {
     double* col = W + j * ldw;
-    double part = 0.0;
-    for (int i = j + 1 + threadIdx.x; i < m; i += TTB_THREADS) part = fma(col[i], col[i], part);
-    double sigma = block_sum(part, red);
-    double alpha = col[j];
+    const double alpha = col[j];
     double t = 0.0, beta = alpha, scale = 0.0;
     if (sigma != 0.0) {
-      double nrm = sqrt(alpha * alpha + sigma);
+      const double nrm = sqrt(alpha * alpha + sigma);
       beta = (alpha >= 0.0) ? -nrm : nrm;
       t = (beta - alpha) / beta;
       scale = 1.0 / (alpha - beta);
     }
     __syncthreads();  // everyone has read col[j] before it is overwritten
     if (sigma != 0.0) {
-      for (int i = j + 1 + threadIdx.x; i < m; i += TTB_THREADS) col[i] *= scale;
+      for (int i = j + 1 + tid; i < m; i += TTB_THREADS) col[i] *= scale;
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       col[j] = beta;
       tau[j] = t;
     }
     __syncthreads();
-    if (t != 0.0) {
-      // trailing update, one warp per column
-      for (int c = j + 1 + wid; c < k; c += TTB_WARPS) {
-        double* cc = W + c * ldw;
-        double w = 0.0;
-        for (int i = j + 1 + lane; i < m; i += 32) w = fma(col[i], cc[i], w);
-        w = warp_sum(w) + cc[j];
-        w *= t;
-        if (lane == 0) cc[j] -= w;
-        for (int i = j + 1 + lane; i < m; i += 32) cc[i] = fma(-w, col[i], cc[i]);
+    double next = 0.0;  // this thread's part of |column j+1, rows > j+1|^2
+    for (int c0 = j + 1; c0 < k; c0 += HC) {
+      const int nc = min(HC, k - c0);
+      double* cb = W + (i64)c0 * ldw;
+      if (t != 0.0) {
+        double w[HC];
+#pragma unroll
+        for (int q = 0; q < HC; ++q) w[q] = 0.0;
+        for (int i = j + 1 + tid; i < m; i += TTB_THREADS) {
+          const double v = col[i];
+#pragma unroll
+          for (int q = 0; q < HC; ++q)
+            if (q < nc) w[q] = fma(v, cb[i + q * ldw], w[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < HC; ++q) {
+          const double sw = warp_sum(w[q]);
+          if (lane == 0) hred[wid][q] = sw;
+        }
+        __syncthreads();
+        if (tid < nc) {
+          double sw = 0.0;
+          for (int q = 0; q < TTB_WARPS; ++q) sw += hred[q][tid];
+          const double wv = t * (sw + cb[j + tid * ldw]);
+          hw[tid] = wv;
+          cb[j + tid * ldw] -= wv;
+        }
+        __syncthreads();
+        for (int i = j + 1 + tid; i < m; i += TTB_THREADS) {
+          const double v = col[i];
+#pragma unroll
+          for (int q = 0; q < HC; ++q) {
+            if (q < nc) {
+              const double x = fma(-hw[q], v, cb[i + q * ldw]);
+              cb[i + q * ldw] = x;
+              if (q == 0 && c0 == j + 1 && i > j + 1) next = fma(x, x, next);
+            }
+          }
+        }
+        __syncthreads();  // hred and hw are reused by the next chunk
+      } else if (c0 == j + 1) {
+        for (int i = j + 2 + tid; i < m; i += TTB_THREADS) next = fma(cb[i], cb[i], next);
       }
     }
-    __syncthreads();
+    if (j + 1 < p) sigma = block_sum(next, red);
   }
 }
 
@@ -899,7 +941,7 @@ static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* t
 constexpr int LNB2 = 64;
 static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, double* W, double* tau,
                                                       Mat R, double* pool, double* red,
-                                                      GemmSmem& gsm) {
+                                                      double* ring) {
   const int p = m < k ? m : k;
   const int tid = threadIdx.x;
   double* G2 = pool;                      // LNB2 x LNB2: V^T V, later T^T Y
@@ -930,9 +972,23 @@ static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, doub
       __syncthreads();
       const int nt = o0 + ob - j0 - jb;
       if (nt > 0) {
-        cta_block_t(Wp, m, rows, jb, tau + j0, Gi, Ti, gsm);
+        // T of the block (as cta_block_t), column by column over the block
+        cta_gemm_pipe(CMat{Wp, m, 1}, CMat{Wp, 1, m}, Mat{Gi, 1, LNB}, jb, jb, rows, 1.0, 0.0,
+                      ring);
+        for (int e = tid; e < LNB * LNB; e += TTB_THREADS) Ti[e] = 0.0;
+        __syncthreads();
+        for (int i = 0; i < jb; ++i) {
+          if (tid < i) {
+            double acc = 0.0;
+            for (int r = tid; r < i; ++r) acc = fma(Ti[tid + r * LNB], Gi[r + i * LNB], acc);
+            Ti[tid + i * LNB] = -tau[j0 + i] * acc;
+          }
+          if (tid == 0) Ti[i + i * LNB] = tau[j0 + i];
+          __syncthreads();
+        }
         double* C = W + j0 + (i64)(j0 + jb) * m;
-        cta_gemm(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Yi, 1, LNB}, jb, nt, rows, 1.0, 0.0, gsm);
+        cta_gemm_pipe(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Yi, 1, LNB}, jb, nt, rows, 1.0, 0.0,
+                      ring);
         for (int col = tid; col < nt; col += TTB_THREADS) {
           double y[LNB];
           for (int i = 0; i < jb; ++i) y[i] = Yi[i + (i64)col * LNB];
@@ -943,7 +999,8 @@ static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, doub
           }
         }
         __syncthreads();
-        cta_gemm(CMat{Wp, 1, m}, CMat{Yi, 1, LNB}, Mat{C, 1, m}, rows, nt, jb, -1.0, 1.0, gsm);
+        cta_gemm_pipe(CMat{Wp, 1, m}, CMat{Yi, 1, LNB}, Mat{C, 1, m}, rows, nt, jb, -1.0, 1.0,
+                      ring);
       }
     }
     // R entries above the inner diagonal blocks move out; V gets zeros there
@@ -958,7 +1015,7 @@ static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, doub
     const int nt = k - o0 - ob;
     if (nt <= 0) continue;
     // T of the panel: T[i, i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V^T V)[0:i, i]
-    cta_gemm(CMat{Wo, m, 1}, CMat{Wo, 1, m}, Mat{G2, 1, LNB2}, ob, ob, orows, 1.0, 0.0, gsm);
+    cta_gemm_pipe(CMat{Wo, m, 1}, CMat{Wo, 1, m}, Mat{G2, 1, LNB2}, ob, ob, orows, 1.0, 0.0, ring);
     for (int e = tid; e < LNB2 * LNB2; e += TTB_THREADS) T2[e] = 0.0;
     __syncthreads();
     for (int i = 0; i < ob; ++i) {
@@ -975,9 +1032,11 @@ static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, doub
       const int nc = min(LNB2, nt - c0);
       double* C = W + o0 + (i64)(o0 + ob + c0) * m;
       // Yo = V^T C, G2 = T^T Yo, C -= V G2
-      cta_gemm(CMat{Wo, m, 1}, CMat{C, 1, m}, Mat{Yo, 1, LNB2}, ob, nc, orows, 1.0, 0.0, gsm);
-      cta_gemm(CMat{T2, LNB2, 1}, CMat{Yo, 1, LNB2}, Mat{G2, 1, LNB2}, ob, nc, ob, 1.0, 0.0, gsm);
-      cta_gemm(CMat{Wo, 1, m}, CMat{G2, 1, LNB2}, Mat{C, 1, m}, orows, nc, ob, -1.0, 1.0, gsm);
+      cta_gemm_pipe(CMat{Wo, m, 1}, CMat{C, 1, m}, Mat{Yo, 1, LNB2}, ob, nc, orows, 1.0, 0.0, ring);
+      cta_gemm_pipe(CMat{T2, LNB2, 1}, CMat{Yo, 1, LNB2}, Mat{G2, 1, LNB2}, ob, nc, ob, 1.0, 0.0,
+                    ring);
+      cta_gemm_pipe(CMat{Wo, 1, m}, CMat{G2, 1, LNB2}, Mat{C, 1, m}, orows, nc, ob, -1.0, 1.0,
+                    ring);
     }
   }
   // the rest of R: below the diagonal zero, right of each outer panel from W
