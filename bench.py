@@ -49,11 +49,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="persistent", choices=["plain", "served", "persistent"])
-    ap.add_argument("--requests", type=int, default=592,
-                    help="requests per step (592 = 4 per SM of a B200)")
+    ap.add_argument("--requests", type=int, default=1184,
+                    help="requests per step (1184 = 8 per SM of a B200)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="requests in the CPU baseline sample (0: automatic)")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="arrival rate of the served run (0: twice the measured batch rate)")
+    ap.add_argument("--plain-sample", type=int, default=8,
+                    help="requests timed through the plain one-at-a-time drop-in (0: skip)")
     ap.add_argument("--diffusion-dims", default="4,5",
                     help="dimensions d the diffusion requests draw from")
     ap.add_argument("--diffusion-modes", default="16,32",
@@ -510,7 +514,15 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     value = ok * world / (total_ms * 1e-3)
-    e2e = e2e_run(eng, reqs, args, torch, flush)
+    e2e = served_run(reqs, args, torch, rate=args.serve_rate or 2.0 * value / world)
+    if world > 1:
+        t = torch.tensor([e2e.pop("_seconds")], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e["value"] = e2e.pop("_solved") * world / float(t.item())
+    else:
+        e2e.pop("_seconds")
+        e2e.pop("_solved")
+    plain = plain_run(reqs, args) if (world == 1 and args.plain_sample > 0) else None
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -541,6 +553,7 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
             "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
             "converged": f"{ok}/{len(reqs) * args.steps}", "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "plain_gpu": plain,
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -581,6 +594,65 @@ def roofline(cls, rec, pk, fp64_tflops):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
             "frac": gbs / peak, "traffic": None, "per_launch_us": 1e3 * rec["ms"] / rec["n"],
             "launches": rec["n"]}
+
+
+def served_run(reqs, args, torch, rate):
+    """End to end through the serving API: the requests (host cores) arrive
+    as a seeded Poisson stream at ``rate`` per second and are served by
+    continuous batching on concurrent persistent launches (inputs copied to
+    the device per launch, solutions read back).  ``args.steps`` passes,
+    each timed with CUDA events around the whole stream."""
+    from ttnumpy_b200.persistent_serving import PersistentServer
+
+    host = [(p.A, p.b, Engine.x0_host(p), solve_kwargs(p)) for p in reqs]
+    rng = np.random.default_rng(args.seed + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    arrivals -= arrivals[0]
+    seconds, solved, lats, launches, h2d, d2h = 0.0, 0, [], 0, 0, 0
+    steps = max(1, args.steps)
+    for _ in range(steps):
+        server = PersistentServer()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        jobs = server.serve(host, list(arrivals))
+        torch.cuda.synchronize()
+        e.record()
+        e.synchronize()
+        seconds += s.elapsed_time(e) * 1e-3
+        solved += sum(1 for j in jobs if j.result.status == 0 and j.result.info.converged)
+        lats.extend(1e3 * j.latency for j in jobs)
+        launches += server.launches
+        h2d, d2h = server.h2d_bytes, server.d2h_bytes
+    return {"value": solved / seconds, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "mode": f"served: {len(reqs)} requests per step arriving as a Poisson stream at "
+                    f"{rate:.1f}/s, continuous batching over 16 streams of persistent launches, "
+                    "inputs copied from host per launch, solutions read back",
+            "launches_per_step": launches / steps,
+            "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
+            "_seconds": seconds, "_solved": solved}
+
+
+def plain_run(reqs, args):
+    """The plain one-solve-at-a-time GPU AMEn (the drop-in ``amen``) on the
+    first requests of the mix, for the served-versus-plain ratio."""
+    import torch
+
+    eng = Engine("plain")
+    sample = reqs[: args.plain_sample]
+    handle = eng.upload(sample)
+    eng.solve_all(handle[:1])
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    results, _ = eng.solve_all(handle)
+    e.record()
+    torch.cuda.synchronize()
+    ok = sum(1 for _, info in results if info.converged)
+    return {"value": ok / (s.elapsed_time(e) * 1e-3), "unit": UNIT,
+            "sample": f"the first {len(sample)} requests of the mix, solved one after another by "
+                      "the drop-in amen (every contraction and factorisation a library call)"}
 
 
 def e2e_run(eng, reqs, args, torch, flush):

@@ -1,0 +1,157 @@
+"""Continuous batching on the persistent whole-solve kernel.
+
+Requests arrive over time.  Whenever one of ``streams`` CUDA streams is
+free and requests are waiting, the waiting requests (at most ``max_batch``,
+longest first) are packed into one persistent launch on that stream
+(``ttb_amen_persistent``: one thread block per solve).  Launches on
+different streams run concurrently, so the blocks of a new launch take the
+SMs that finished solves of earlier launches leave idle: a short request
+does not wait for the longest solve of an earlier batch.  Each launch copies
+its requests' inputs from host memory on its own stream and the solutions
+are read back when its completion event has fired.
+
+A request whose bonds outgrow the launch's slot capacity (status -4) is
+queued again with twice the capacity, as ``amen_persistent`` does.
+Latency is measured per request on the host clock, from arrival to the
+moment its launch is found complete.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from typing import Callable, List, Optional, Sequence
+
+import torch
+
+from . import kernels as K
+from .persistent import PersistentBatch, Result, _cost, _Prepared
+
+
+@dataclass
+class Job:
+    rid: int
+    arrival: float
+    prep: _Prepared
+    rmax: int
+    result: Optional[Result] = None
+    done_at: Optional[float] = None
+    host_cores: Optional[list] = None  # the solution's cores read back to the host
+
+    @property
+    def latency(self) -> Optional[float]:
+        return None if self.done_at is None else self.done_at - self.arrival
+
+
+class PersistentServer:
+    """Serve AMEn requests with concurrent persistent launches.
+
+    ``streams`` bounds the launches in flight, ``max_batch`` the requests of
+    one launch; a launch is issued at most every ``min_interval`` seconds
+    unless ``max_batch`` requests are waiting, so arrivals in a burst share
+    a launch.
+    """
+
+    def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: int = 64,
+                 max_rmax: int = 256, min_interval: float = 0.005, download: bool = True):
+        K.device_ok()
+        self.streams = [torch.cuda.Stream() for _ in range(streams)]
+        self.free = list(range(streams))
+        self.max_batch = max_batch
+        self.rmax = rmax
+        self.max_rmax = max_rmax
+        self.min_interval = min_interval
+        self.download = download
+        self.queue: List[Job] = []
+        self.inflight = []  # (stream index, batch, event, jobs)
+        self.completed: List[Job] = []
+        self.launches = 0
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+        self._last_launch = -1e30
+
+    def submit(self, rid: int, arrival: float, A, b, x0=None, kwargs: Optional[dict] = None) -> Job:
+        """Validate a request on the host and queue it (``amen`` arguments)."""
+        job = Job(rid, arrival, _Prepared(A, b, x0, dict(kwargs or {})), self.rmax)
+        self.queue.append(job)
+        return job
+
+    def _launch(self, now: float) -> bool:
+        if not self.queue or not self.free:
+            return False
+        if len(self.queue) < self.max_batch and now - self._last_launch < self.min_interval:
+            return False
+        rmax = min(j.rmax for j in self.queue)
+        take = [j for j in self.queue if j.rmax == rmax][: self.max_batch]
+        taken = set(id(j) for j in take)
+        self.queue = [j for j in self.queue if id(j) not in taken]
+        take.sort(key=lambda j: -_cost(j.prep))
+        si = self.free.pop()
+        s = self.streams[si]
+        with torch.cuda.stream(s):
+            batch = PersistentBatch([j.prep for j in take], rmax)
+            batch.launch(s)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self.h2d_bytes += batch.h2d_bytes
+        self.inflight.append((si, batch, ev, take))
+        self.launches += 1
+        self._last_launch = now
+        return True
+
+    def _collect(self, now: float) -> bool:
+        done_any = False
+        still = []
+        for si, batch, ev, jobs in self.inflight:
+            if not ev.query():
+                still.append((si, batch, ev, jobs))
+                continue
+            done_any = True
+            with torch.cuda.stream(self.streams[si]):
+                results = batch.collect()
+                for job, res in zip(jobs, results):
+                    if res.status == -4 and job.rmax < self.max_rmax:
+                        job.rmax = min(2 * job.rmax, self.max_rmax)
+                        self.queue.append(job)
+                        continue
+                    job.result = res
+                    if self.download and res.x is not None:
+                        job.host_cores = res.x.to_numpy()
+                        self.d2h_bytes += sum(c.nbytes for c in job.host_cores)
+                    job.done_at = now
+                    self.completed.append(job)
+            self.free.append(si)
+        self.inflight = still
+        return done_any
+
+    def step(self, now: float) -> bool:
+        """Collect finished launches, then issue new ones; True if anything
+        happened."""
+        a = self._collect(now)
+        b = False
+        while self._launch(now):
+            b = True
+        return a or b
+
+    def idle(self) -> bool:
+        return not self.queue and not self.inflight
+
+    def serve(self, requests: Sequence, arrivals: Sequence[float],
+              clock: Callable[[], float] = time.perf_counter) -> List[Job]:
+        """Submit ``requests`` [(A, b, x0, kwargs)] at ``arrivals`` (seconds
+        from the start) and serve them to completion; returns the jobs in
+        request order."""
+        order = sorted(range(len(requests)), key=lambda i: arrivals[i])
+        jobs: List[Optional[Job]] = [None] * len(requests)
+        t0 = clock()
+        nxt = 0
+        while nxt < len(order) or not self.idle():
+            now = clock() - t0
+            while nxt < len(order) and arrivals[order[nxt]] <= now:
+                i = order[nxt]
+                A, b, x0, kw = requests[i]
+                jobs[i] = self.submit(i, arrivals[i], A, b, x0, kw)
+                nxt += 1
+            if not self.step(clock() - t0):
+                time.sleep(0.0005)
+        return jobs
