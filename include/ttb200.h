@@ -69,6 +69,16 @@ typedef struct {
 } ttb_gemm_t;
 int ttb_gemm(const ttb_gemm_t* problems, int count, void* stream);
 
+/* The same products on the tcgen05 tensor cores in mixed precision (no
+ * counterpart in the reference, which multiplies in float64 throughout):
+ * every float64 operand element is split into two TF32 parts (hi, lo) and
+ * the three leading products hi*hi + hi*lo + lo*hi are accumulated in FP32
+ * in tensor memory, then scaled into C in float64.  Relative accuracy about
+ * 1e-6 of |A| |B| (22-bit operand parts, FP32 accumulation).  ``status``
+ * (device int, may be NULL) is set to 1 if a block gave up waiting on the
+ * tensor core (its tile of C is then left unwritten). */
+int ttb_gemm_3xtf32(const ttb_gemm_t* problems, int count, int* status, void* stream);
+
 /* ------------------------------------------------------------------------
  * Environment update: one step of the left or right projection recursion,
  * replacing prepare_left_environment / prepare_right_environment

@@ -126,6 +126,7 @@ _SIGNATURES = {
     "ttb_local_apply": ([C.POINTER(Local), I, P], I),
     "ttb_local_matrix": ([C.POINTER(LocalMatrix), I, P], I),
     "ttb_project": ([C.POINTER(Project), I, P], I),
+    "ttb_gemm_3xtf32": ([C.POINTER(Gemm), I, P, P], I),
     "ttb_qr_work_doubles": ([I, I], L),
     "ttb_qr": ([C.POINTER(QR), I, P], I),
     "ttb_qr_static": ([C.POINTER(QR), I, P], I),

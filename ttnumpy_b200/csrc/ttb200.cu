@@ -1340,6 +1340,10 @@ int qr_static_base(double** out) {
 
 }  // namespace
 
+namespace ttb {
+void count_launch() { counted(); }
+}  // namespace ttb
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

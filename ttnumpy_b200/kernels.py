@@ -129,6 +129,16 @@ def gemm_many(descs: Sequence) -> None:
     check(lib().ttb_gemm(arr, len(descs), stream()), "ttb_gemm")
 
 
+def gemm_3xtf32_many(descs: Sequence, status: Optional[torch.Tensor] = None) -> None:
+    """The ttb_gemm problems on the tcgen05 tensor cores in 3xTF32
+    (about 1e-6 relative accuracy); ``status`` (int32 device tensor) is set
+    to 1 if a block gave up waiting on the tensor core."""
+    if not descs:
+        return
+    arr = (_lib.Gemm * len(descs))(*descs)
+    check(lib().ttb_gemm_3xtf32(arr, len(descs), ptr(status), stream()), "ttb_gemm_3xtf32")
+
+
 def gemm(a, b, c, alpha=1.0, beta=0.0) -> torch.Tensor:
     gemm_many([gemm_desc(a, b, c, alpha, beta)])
     return c
