@@ -363,7 +363,7 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   double* Y = c.pool;
   double* G = Y + (i64)LNB * YCH;
   double* Tm = G + LNB * LNB;
-  cta_qr_blocked(A, m, k, W, W + (i64)m * k, Q, R, Y, G, Tm, c.sm->red, *c.gsm);
+  cta_qr_blocked(A, m, k, W, W + (i64)m * k, Q, R, Y, G, Tm, c.sm->red, *c.gsm, c.ring);
   c.top = mark;
 }
 
@@ -398,7 +398,7 @@ __device__ __noinline__ void svd(Ctx& c, CMat A, int m, int k, Mat U, double* S,
     double* G = Y + (i64)LNB * YCH;
     double* Tm = G + LNB * LNB;
     cta_svd_tall_blocked(At, M, K, W, tau, Bsq, V, sv, order, flag, Ut, S, Vt, Y, G, Tm,
-                         c.sm->red, *c.gsm);
+                         c.sm->red, *c.gsm, c.ring);
   }
   c.top = mark;
 }
@@ -462,7 +462,7 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
     __syncthreads();
     if (info == 0) vcopy(u, bb, N);
   } else {
-    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, *c.gsm);
+    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, *c.gsm, c.ring);
   }
   __syncthreads();
   if (info != 0) c.status = ST_SINGULAR;

@@ -357,6 +357,18 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
   __syncthreads();  // callers may reuse the ring and read C right away
 }
 
+// The blocked factorisations take an optional GEMM ring: with one, their
+// trailing-update products are pipelined (cta_gemm_pipe), else they use the
+// one-stage tile in ``gsm``.
+static __device__ __forceinline__ void gemm_sel(CMat A, CMat B, OMat C, int M, int N, int K,
+                                                double alpha, double beta, GemmSmem& gsm,
+                                                double* ring) {
+  if (ring)
+    cta_gemm_pipe(A, B, C, M, N, K, alpha, beta, ring);
+  else
+    cta_gemm(A, B, C, M, N, K, alpha, beta, gsm);
+}
+
 // ---------------------------------------------------------------------------
 // copies
 // ---------------------------------------------------------------------------
@@ -719,7 +731,7 @@ constexpr int YCH = 512;  // columns per chunk of the blocked trailing updates
 // (rows x LNB doubles, shared or global memory), trailing updates as GEMMs.
 // Same pivot rule and result as cta_gepp_solve; b becomes the solution.
 static __device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, double* panel, double* redv,
-                                int* redi, int* ipiv, GemmSmem& gsm) {
+                                int* redi, int* ipiv, GemmSmem& gsm, double* ring = nullptr) {
   const int tid = threadIdx.x;
   for (int j0 = 0; j0 < n; j0 += LNB) {
     const int jb = min(LNB, n - j0);
@@ -787,9 +799,9 @@ static __device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, doub
     if (rows > jb) {
       // A22 -= L21 U12 ; b2 -= L21 u_b
       if (ncols > 0)
-        cta_gemm(CMat{P + jb, 1, rows}, CMat{W + j0 + (i64)(j0 + jb) * ld, 1, ld},
+        gemm_sel(CMat{P + jb, 1, rows}, CMat{W + j0 + (i64)(j0 + jb) * ld, 1, ld},
                  Mat{W + (j0 + jb) + (i64)(j0 + jb) * ld, 1, ld}, rows - jb, ncols, jb, -1.0,
-                 1.0, gsm);
+                 1.0, gsm, ring);
       for (int i = tid; i < rows - jb; i += TTB_THREADS) {
         double acc = b[j0 + jb + i];
         for (int q = 0; q < jb; ++q) acc = fma(-P[jb + i + (i64)q * rows], b[j0 + q], acc);
@@ -813,8 +825,8 @@ static __device__ int cta_gepp_blocked(double* W, i64 ld, double* b, int n, doub
 // reflector block (unit diagonal, zeros above) in Wp with leading dim ldw
 // (LAPACK dlarft, forward column-wise).  G is jb x jb scratch.
 static __device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, const double* tau,
-                            double* G, double* Tm, GemmSmem& gsm) {
-  cta_gemm(CMat{Wp, ldw, 1}, CMat{Wp, 1, ldw}, Mat{G, 1, LNB}, jb, jb, rows, 1.0, 0.0, gsm);
+                            double* G, double* Tm, GemmSmem& gsm, double* ring = nullptr) {
+  gemm_sel(CMat{Wp, ldw, 1}, CMat{Wp, 1, ldw}, Mat{G, 1, LNB}, jb, jb, rows, 1.0, 0.0, gsm, ring);
   if (threadIdx.x == 0) {
     for (int i = 0; i < jb; ++i) {
       for (int q = 0; q < i; ++q) {
@@ -834,19 +846,19 @@ static __device__ void cta_block_t(const double* Wp, i64 ldw, int rows, int jb, 
 // applied last block first; only rows >= the block's first row change.
 // Columns of X left of a block are untouched (as for an identity start).
 static __device__ void cta_apply_q_blocked(const double* W, int m, int p, const double* tau, Mat X,
-                                    int nx, double* Y, double* G, double* Tm, GemmSmem& gsm) {
+                                    int nx, double* Y, double* G, double* Tm, GemmSmem& gsm, double* ring = nullptr) {
   const int tid = threadIdx.x;
   const int last = ((p - 1) / LNB) * LNB;
   for (int j0 = last; j0 >= 0; j0 -= LNB) {
     const int jb = min(LNB, p - j0);
     const int rows = m - j0;
     const double* Wp = W + j0 + (i64)j0 * m;
-    cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm);
+    cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm, ring);
     for (int c0 = 0; c0 < nx; c0 += YCH) {
       const int nc = min(YCH, nx - c0);
       Mat Xs{X.p + j0 * X.rs + c0 * X.cs, X.rs, X.cs};
-      cta_gemm(CMat{Wp, m, 1}, CMat{Xs.p, Xs.rs, Xs.cs}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0,
-               gsm);
+      gemm_sel(CMat{Wp, m, 1}, CMat{Xs.p, Xs.rs, Xs.cs}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0,
+               gsm, ring);
       for (int col = tid; col < nc; col += TTB_THREADS) {
         double y[LNB];
         for (int i = 0; i < jb; ++i) y[i] = Y[i + (i64)col * LNB];
@@ -857,7 +869,7 @@ static __device__ void cta_apply_q_blocked(const double* W, int m, int p, const 
         }
       }
       __syncthreads();
-      cta_gemm(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Xs, rows, nc, jb, -1.0, 1.0, gsm);
+      gemm_sel(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Xs, rows, nc, jb, -1.0, 1.0, gsm, ring);
     }
   }
 }
@@ -869,7 +881,7 @@ static __device__ void cta_apply_q_blocked(const double* W, int m, int p, const 
 // and R (p x k) as in cta_qr; either may be NULL.  Same reflectors and R as
 // the unblocked factorisation up to rounding.
 static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* tau, Mat Q, Mat R,
-                               double* Y, double* G, double* Tm, double* red, GemmSmem& gsm) {
+                               double* Y, double* G, double* Tm, double* red, GemmSmem& gsm, double* ring = nullptr) {
   const int p = m < k ? m : k;
   const int tid = threadIdx.x;
   cta_copy(A, Mat{W, 1, (i64)m}, m, k);
@@ -890,12 +902,12 @@ static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* t
     __syncthreads();
     const int nt = k - j0 - jb;
     if (nt > 0) {
-      cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm);
+      cta_block_t(Wp, m, rows, jb, tau + j0, G, Tm, gsm, ring);
       for (int c0 = 0; c0 < nt; c0 += YCH) {
         const int nc = min(YCH, nt - c0);
         double* C = W + j0 + (i64)(j0 + jb + c0) * m;
         // Y = V^T C (jb x nc), then Y = T^T Y, then C -= V Y
-        cta_gemm(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0, gsm);
+        gemm_sel(CMat{Wp, m, 1}, CMat{C, 1, m}, Mat{Y, 1, LNB}, jb, nc, rows, 1.0, 0.0, gsm, ring);
         for (int col = tid; col < nc; col += TTB_THREADS) {
           double y[LNB];
           for (int i = 0; i < jb; ++i) y[i] = Y[i + (i64)col * LNB];
@@ -906,7 +918,7 @@ static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* t
           }
         }
         __syncthreads();
-        cta_gemm(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Mat{C, 1, m}, rows, nc, jb, -1.0, 1.0, gsm);
+        gemm_sel(CMat{Wp, 1, m}, CMat{Y, 1, LNB}, Mat{C, 1, m}, rows, nc, jb, -1.0, 1.0, gsm, ring);
       }
     }
   }
@@ -925,7 +937,7 @@ static __device__ void cta_qr_blocked(CMat A, int m, int k, double* W, double* t
       Q(i, j) = (i == j) ? 1.0 : 0.0;
     }
     __syncthreads();
-    cta_apply_q_blocked(W, m, p, tau, Q, p, Y, G, Tm, gsm);
+    cta_apply_q_blocked(W, m, p, tau, Q, p, Y, G, Tm, gsm, ring);
   }
   __syncthreads();
 }
@@ -1058,8 +1070,8 @@ static __device__ __noinline__ void cta_qr_r_blocked2(CMat A, int m, int k, doub
 static __device__ int cta_svd_tall_blocked(CMat A, int m, int k, double* W, double* tau, double* Bsq,
                                     double* V, double* sv, int* order, int* flag, Mat U, double* S,
                                     Mat Vh, double* Y, double* G, double* Tm, double* red,
-                                    GemmSmem& gsm) {
-  cta_qr_blocked(A, m, k, W, tau, Mat{nullptr, 0, 0}, Mat{Bsq, 1, (i64)k}, Y, G, Tm, red, gsm);
+                                    GemmSmem& gsm, double* ring = nullptr) {
+  cta_qr_blocked(A, m, k, W, tau, Mat{nullptr, 0, 0}, Mat{Bsq, 1, (i64)k}, Y, G, Tm, red, gsm, ring);
   __syncthreads();
   const double tol = 4.0 * k * 2.220446049250313e-16;
   int status = cta_jacobi(Bsq, k, k, V, k, 60, tol, flag);
@@ -1094,7 +1106,7 @@ static __device__ int cta_svd_tall_blocked(CMat A, int m, int k, double* W, doub
     Vh(r, c) = V[c + (i64)order[r] * k];
   }
   __syncthreads();
-  cta_apply_q_blocked(W, m, k, tau, U, k, Y, G, Tm, gsm);
+  cta_apply_q_blocked(W, m, k, tau, U, k, Y, G, Tm, gsm, ring);
   return status;
 }
 

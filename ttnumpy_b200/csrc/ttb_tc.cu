@@ -124,30 +124,30 @@ __device__ __forceinline__ void stage_in(const TcDesc& q, const double* A, const
   float* alo = st + A_FL;
   float* bhi = st + 2 * A_FL;
   float* blo = st + 2 * A_FL + B_FL;
+  // element e lands at float e of its plane: each warp fills one 8-row x
+  // 4-column core matrix (lane -> row lane / 4, column lane % 4), so the
+  // shared-memory stores are contiguous and the global loads read 4
+  // neighbouring columns of 8 rows
   const int tid = threadIdx.x;
-  const bool a_kfast = (q.a_cs == 1);
   for (int e = tid; e < TM * TK; e += THREADS) {
-    int r, c;
-    if (a_kfast) { c = e % TK; r = e / TK; } else { r = e % TM; c = e / TM; }
+    const int u = e >> 5, ln = e & 31;
+    const int r = (u % (TM / 8)) * 8 + (ln >> 2), c = (u / (TM / 8)) * 4 + (ln & 3);
     const int gm = m0 + r, gk = k0 + c;
     const double x = (gm < q.m && gk < q.k) ? A[gm * q.a_rs + gk * q.a_cs] : 0.0;
     float hi, lo;
     split_tf32(x, hi, lo);
-    const int idx = (((c >> 2) * (TM / 8) + (r >> 3)) * 8 + (r & 7)) * 4 + (c & 3);
-    ahi[idx] = hi;
-    alo[idx] = lo;
+    ahi[e] = hi;
+    alo[e] = lo;
   }
-  const bool b_nfast = (q.b_cs == 1);
   for (int e = tid; e < TN * TK; e += THREADS) {
-    int j, c;
-    if (b_nfast) { j = e % TN; c = e / TN; } else { c = e % TK; j = e / TK; }
+    const int u = e >> 5, ln = e & 31;
+    const int j = (u % (TN / 8)) * 8 + (ln >> 2), c = (u / (TN / 8)) * 4 + (ln & 3);
     const int gn = n0 + j, gk = k0 + c;
     const double x = (gn < q.n && gk < q.k) ? B[gk * q.b_rs + gn * q.b_cs] : 0.0;
     float hi, lo;
     split_tf32(x, hi, lo);
-    const int idx = (((c >> 2) * (TN / 8) + (j >> 3)) * 8 + (j & 7)) * 4 + (c & 3);
-    bhi[idx] = hi;
-    blo[idx] = lo;
+    bhi[e] = hi;
+    blo[e] = lo;
   }
 }
 
