@@ -93,15 +93,16 @@ def make_requests(count: int, seed: int, dims=(4, 5), modes=(16, 32)):
     return reqs
 
 
-# DRAM bytes (read + write) of one k_amen launch of the default workload,
-# from an ncu capture of `python bench.py`; other workloads report null
-DEFAULT_TRAFFIC = 655255445760 + 720370022144
+# DRAM bytes (read + write) of one k_amen launch of the standard mix at
+# 1184 and 592 requests per step, from ncu captures of `python bench.py`
+# (profiles/k_amen_bench_*req.md); other workloads report null
+MEASURED_TRAFFIC = {1184: 1658012785152 + 1601813339392, 592: 655255445760 + 720370022144}
 
 
 def _traffic(args):
-    default = (args.requests == 592 and args.seed == 0 and _ints(args.diffusion_dims) == [4, 5]
-               and _ints(args.diffusion_modes) == [16, 32])
-    return DEFAULT_TRAFFIC if default else None
+    standard = (args.seed == 0 and _ints(args.diffusion_dims) == [4, 5]
+                and _ints(args.diffusion_modes) == [16, 32])
+    return MEASURED_TRAFFIC.get(args.requests) if standard else None
 
 
 def _ints(text):
@@ -534,7 +535,7 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
             "(ttb_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
             "frac": ach / fp64, "traffic": _traffic(args),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
-                              "this workload (profiles/k_amen_bench_592req.md)",
+                              f"this workload (profiles/k_amen_bench_{args.requests}req.md)",
             "flops_counted": "2mnk of every dense product the blocks ran; QR/SVD/LU not counted",
             "per_launch_us": 1e3 * sum(step_ms) / len(step_ms), "launches": len(step_ms)}
     cpu = None
