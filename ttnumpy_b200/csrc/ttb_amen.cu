@@ -16,6 +16,10 @@
 #include "ttb200.h"
 #include "ttb_device.cuh"
 
+namespace ttb {
+void count_launch();  // the library's launch counter (ttb200.cu)
+}
+
 namespace {
 
 using namespace ttb;
@@ -1482,6 +1486,7 @@ int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void*
     configured = 1;
   }
   k_amen<<<count, TTB_THREADS, smem, reinterpret_cast<cudaStream_t>(stream)>>>(tasks, rmax);
+  ttb::count_launch();
   return (int)cudaGetLastError();
 }
 
