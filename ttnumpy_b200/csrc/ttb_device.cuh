@@ -87,18 +87,24 @@ struct CMat {
 };
 
 // ---------------------------------------------------------------------------
-// GEMM: one 64x64 output tile per call, K staged through shared memory,
+// GEMM: one GBM x 64 output tile per call, K staged through shared memory,
 // products on the FP64 tensor-core path (mma.sync m8n8k4 .f64)
 // ---------------------------------------------------------------------------
 
-constexpr int GBM = 64, GBN = 64, GBK = 16;
-// Row pitch of the staged tiles: 68 doubles puts the four k-rows a fragment
-// load touches on disjoint bank groups, so each load takes two wavefronts.
-constexpr int GPITCH = 68;
+// Tile rows: 32 per four warps (64 for 8 warps, 96 for 12), 64 columns.
+constexpr int GBM = 8 * TTB_WARPS, GBN = 64, GBK = 16;
+// Row pitches of the staged tiles: 4 more than a multiple of 16 doubles puts
+// the four k-rows a fragment load touches on disjoint bank groups, so each
+// load takes two wavefronts.
+constexpr int GPITCH_A = GBM + 4, GPITCH_B = GBN + 4;
+// loads per thread of one k-step's A and B tiles
+constexpr int GNA = (GBM * GBK) / TTB_THREADS;
+constexpr int GNB = (GBK * GBN + TTB_THREADS - 1) / TTB_THREADS;
+static_assert(GNA * TTB_THREADS == GBM * GBK, "A tile loads must divide evenly");
 
 struct GemmSmem {
-  double a[GBK][GPITCH];  // a[k][m]
-  double b[GBK][GPITCH];  // b[k][n]
+  double a[GBK][GPITCH_A];  // a[k][m]
+  double b[GBK][GPITCH_B];  // b[k][n]
 };
 
 // D += A(8x4, row) * B(4x8, col) in FP64; lane l holds A[l/4][l%4],
@@ -132,9 +138,10 @@ struct OMat {
   }
 };
 
-// C[m0:m0+64, n0:n0+64] = alpha * A * B + beta * C over the full K range.
-// A is M x K, B is K x N.  beta == 0 never reads C.  The eight warps form a
-// 2 x 4 grid of 32 x 16 warp tiles, each 4 x 2 MMA tiles of 8 x 8.
+// C[m0:m0+GBM, n0:n0+64] = alpha * A * B + beta * C over the full K range.
+// A is M x K, B is K x N.  beta == 0 never reads C.  The warps form a
+// (TTB_WARPS / 4) x 4 grid of 32 x 16 warp tiles, each 4 x 2 MMA tiles of
+// 8 x 8 (the tile is GBM = 8 * TTB_WARPS rows by 64 columns).
 static __device__ void cta_gemm_tile(CMat A, CMat B, const OMat& C, int M, int N, int K, int m0,
                                      int n0, double alpha, double beta, GemmSmem& sm) {
   const int tid = threadIdx.x;
@@ -150,15 +157,20 @@ static __device__ void cta_gemm_tile(CMat A, CMat B, const OMat& C, int M, int N
   // loads walk the unit-stride direction of each operand when there is one
   const bool a_kfast = (A.cs == 1);
   const bool b_nfast = (B.cs == 1) || (B.rs != 1);
-  double ra[4], rb[4];
+  double ra[GNA], rb[GNB];
   auto load = [&](int k0) {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < GNA; ++e) {
       int idx = tid + e * TTB_THREADS;
       int mm, kk;
       if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
       int gm = m0 + mm, gk = k0 + kk;
       ra[e] = (gm < M && gk < K) ? A(gm, gk) : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < GNB; ++e) {
+      int idx = tid + e * TTB_THREADS;
+      if (idx >= GBK * GBN) break;
       int nn, kb;
       if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
       int gn = n0 + nn, gk2 = k0 + kb;
@@ -167,11 +179,16 @@ static __device__ void cta_gemm_tile(CMat A, CMat B, const OMat& C, int M, int N
   };
   auto store = [&]() {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < GNA; ++e) {
       int idx = tid + e * TTB_THREADS;
       int mm, kk;
       if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
       sm.a[kk][mm] = ra[e];
+    }
+#pragma unroll
+    for (int e = 0; e < GNB; ++e) {
+      int idx = tid + e * TTB_THREADS;
+      if (idx >= GBK * GBN) break;
       int nn, kb;
       if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
       sm.b[kb][nn] = rb[e];
@@ -234,13 +251,13 @@ static __device__ __noinline__ void cta_gemm(CMat A, CMat B, OMat C, int M, int 
 // stages.  The (output tile, k-tile) steps of the whole product form one
 // sequence, so loads run GSTAGES - 1 steps ahead across tile boundaries and
 // a tile's first operands arrive while the previous tile is finishing.
-// ``ring`` holds GSTAGES * 2 * GBK * GPITCH doubles of shared memory; its
+// ``ring`` holds GSTAGES * GSTAGE_D doubles of shared memory; its
 // first stage has the layout of GemmSmem.  A and B may be anywhere (shared
 // operands take the one-stage path); C must not overlap the ring.
 // ---------------------------------------------------------------------------
 
 constexpr int GSTAGES = 3;
-constexpr int GSTAGE_D = 2 * GBK * GPITCH;
+constexpr int GSTAGE_D = GBK * (GPITCH_A + GPITCH_B);
 
 static __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -281,20 +298,25 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
       const int tile = step / nk, kt = step % nk;
       const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN, k0 = kt * GBK;
       double* sa = ring + (step % GSTAGES) * GSTAGE_D;
-      double* sb = sa + GBK * GPITCH;
+      double* sb = sa + GBK * GPITCH_A;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
+      for (int e = 0; e < GNA; ++e) {
         const int idx = tid + e * TTB_THREADS;
         int mm, kk;
         if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
         const int gm = m0 + mm, gk = k0 + kk;
         const bool oka = gm < M && gk < K;
-        cp_async8(sa + kk * GPITCH + mm, oka ? A.p + gm * A.rs + gk * A.cs : A.p, oka);
+        cp_async8(sa + kk * GPITCH_A + mm, oka ? A.p + gm * A.rs + gk * A.cs : A.p, oka);
+      }
+#pragma unroll
+      for (int e = 0; e < GNB; ++e) {
+        const int idx = tid + e * TTB_THREADS;
+        if (idx >= GBK * GBN) break;
         int nn, kb;
         if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
         const int gn = n0 + nn, gk2 = k0 + kb;
         const bool okb = gn < N && gk2 < K;
-        cp_async8(sb + kb * GPITCH + nn, okb ? B.p + gk2 * B.rs + gn * B.cs : B.p, okb);
+        cp_async8(sb + kb * GPITCH_B + nn, okb ? B.p + gk2 * B.rs + gn * B.cs : B.p, okb);
       }
     }
     cp_async_commit();
@@ -314,14 +336,14 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
     __syncthreads();  // this step's operands landed; the previous step's reads are done
     issue(step + GSTAGES - 1);
     const double* sa = ring + (step % GSTAGES) * GSTAGE_D;
-    const double* sb = sa + GBK * GPITCH;
+    const double* sb = sa + GBK * GPITCH_A;
 #pragma unroll
     for (int kk = 0; kk < GBK; kk += 4) {
       double av[4], bv[2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * GPITCH + wm + 8 * i + g];
+      for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * GPITCH_A + wm + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) bv[j] = sb[(kk + t) * GPITCH + wn + 8 * j + g];
+      for (int j = 0; j < 2; ++j) bv[j] = sb[(kk + t) * GPITCH_B + wn + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
