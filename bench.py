@@ -105,6 +105,22 @@ def _traffic(args):
     return MEASURED_TRAFFIC.get(args.requests) if standard else None
 
 
+def aggregate_rate(solved: int, ms: float, world: int, device: str = "cuda"):
+    """Whole-job rate over the ranks: all ranks' solves over the slowest
+    rank's time.  Returns (solves per second, max milliseconds); a single
+    process needs no process group."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([float(solved), float(ms)], dtype=torch.float64, device=device)
+        mx = t.clone()
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        solved, ms = float(t[0].item()), float(mx[1].item())
+    return solved / (ms * 1e-3), ms
+
+
 def _ints(text):
     return [int(v) for v in str(text).split(",") if v.strip()]
 
@@ -442,13 +458,7 @@ def main():
         lib.ttb_profile_enable(0)
     barrier()
     dom = profile_read(lib)[dominant]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    solved = ok * world
-    value = solved / (total_ms * 1e-3)
+    value, total_ms = aggregate_rate(ok, sum(step_ms), world)
 
     # end to end through the public API from pinned host buffers
     e2e = e2e_run(eng, reqs, args, torch, flush)
@@ -509,20 +519,9 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
             lats.extend(batch.latencies_ms())
             flops += batch.gemm_flops()
     barrier()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = ok * world / (total_ms * 1e-3)
+    value, total_ms = aggregate_rate(ok, sum(step_ms), world)
     e2e = served_run(reqs, args, torch, rate=args.serve_rate or 2.0 * value / world)
-    if world > 1:
-        t = torch.tensor([e2e.pop("_seconds")], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e["value"] = e2e.pop("_solved") * world / float(t.item())
-    else:
-        e2e.pop("_seconds")
-        e2e.pop("_solved")
+    e2e["value"], _ = aggregate_rate(e2e.pop("_solved"), 1e3 * e2e.pop("_seconds"), world)
     plain = plain_run(reqs, args) if (world == 1 and args.plain_sample > 0) else None
     if rank != 0:
         if world > 1:
