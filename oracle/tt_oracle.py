@@ -765,3 +765,58 @@ def amen(A: Train, b: Train, x0: Optional[Train] = None, kickrank=4, error_thres
         orthonormalize(x, "left", center_position=redundant[-1])
         orthonormalize(x, "right", center_position=0)
     return x, info
+
+
+def als(A: Train, b: Train, x0: Optional[Train] = None, max_sweeps=4, residual_tol=None,
+        stagnation_factor="auto", local_solver="auto", direct_solve_size=1000, local_rtol=None,
+        allow_dense_fallback=False, symmetric=False, return_info=True):
+    """ALS one-site sweeps (``solvers/als.py:57-212``): AMEn's local solves
+    and centre shifts without the residual train, enrichment or truncation,
+    so the bonds of ``x0`` never change.  Returns ``(x, info)``; the
+    per-sweep monitor is the one of ``amen`` (``solvers/common.py:504-592``).
+    """
+    d = len(A)
+    st = resolve_settings(max_sweeps, residual_tol, stagnation_factor, local_solver, symmetric,
+                          direct_solve_size, return_info, local_rtol, allow_dense_fallback, 1)
+    if x0 is None:
+        x0 = ones(b.row_modes, ranks=b.bonds)
+    x = x0.copy()
+    if x.orth_center != 0:
+        orthonormalize(x, "right")
+    E = {name: [None] * d for name in ("lA", "rA", "lb", "rb")}
+    for i in range(d - 1, -1, -1):  # als.py:144-146
+        env_right(E["rA"], i, x, x, A)
+        env_right(E["rb"], i, x, b)
+    info = Info()
+    b_norm = tt_norm(b) if st.track_residual else None
+    for sweep in range(st.max_sweeps):
+        for k in range(d - 1):  # als.py:153-170
+            env_left(E["lA"], k, x, x, A)
+            env_left(E["lb"], k, x, b)
+            u, _, _ = _local_solve_one_site(k, x, A, b, E["lA"], E["rA"], E["lb"], E["rb"], st, info)
+            shift_right(x, k, u.reshape(x.bonds[k], x.row_modes[k], x.bonds[k + 1]))
+        env_left(E["lA"], d - 1, x, x, A)  # als.py:172-175
+        env_left(E["lb"], d - 1, x, b)
+        for k in range(d - 1, -1, -1):  # als.py:177-201
+            env_right(E["rA"], k, x, x, A)
+            env_right(E["rb"], k, x, b)
+            u, _, _ = _local_solve_one_site(k, x, A, b, E["lA"], E["rA"], E["lb"], E["rb"], st, info)
+            core = u.reshape(x.bonds[k], x.row_modes[k], x.bonds[k + 1])
+            if k == 0:
+                x.cores[0] = core.reshape(core.shape[0], core.shape[1], 1, core.shape[2])
+                x.orth_center = 0
+            else:
+                shift_left(x, k, core)
+        info.num_sweeps_run = sweep + 1
+        info.max_bonds.append(max(x.bonds))
+        if st.track_residual:
+            res = relative_residual(A, b, x, b_norm=b_norm)
+            info.residuals.append(res)
+            if st.residual_tol is not None and res <= st.residual_tol:
+                info.stop_reason = "converged"
+                break
+            if (st.stagnation_factor is not None and len(info.residuals) >= 2
+                    and info.residuals[-1] > st.stagnation_factor * info.residuals[-2]):
+                info.stop_reason = "stagnated"
+                break
+    return x, info

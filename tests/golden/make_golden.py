@@ -3,7 +3,8 @@
 Run from the repository root, in a checkout that has the reference project
 next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every case
+    python tests/golden/make_golden.py als      # the ALS cases only
 
 Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
 cores as ``<train>_<k>`` arrays plus ``<train>_n``), the call's arguments
@@ -58,15 +59,15 @@ def save(name: str, data: dict, args: dict) -> None:
     print(f"{name}: {size / 1024:.1f} KiB")
 
 
-def amen_case(name, A, b, x0=None, full=True, **kw):
-    """Run the reference amen and store inputs plus outputs."""
+def amen_case(name, A, b, x0=None, full=True, solver=None, **kw):
+    """Run the reference amen (or ``solver``) and store inputs plus outputs."""
     data = {}
     pack(data, "A", A)
     pack(data, "b", b)
     if x0 is not None:
         pack(data, "x0", x0)
     t0 = time.perf_counter()
-    x, info = tt.amen(A, b, x0=x0, return_info=True, **kw)
+    x, info = (solver or tt.amen)(A, b, x0=x0, return_info=True, **kw)
     elapsed = time.perf_counter() - t0
     pack(data, "x", x)
     data["residuals"] = np.array(info.residuals, dtype=np.float64)
@@ -96,7 +97,35 @@ def qtt_laplacian_1d(order):
     return A, lap
 
 
+def als_cases() -> None:
+    """ALS (ttnumpy/solvers/als.py), the next solver on the path: fixed
+    ranks, no enrichment."""
+    from ttnumpy.solvers.als import als
+
+    # QTT Laplacian with a rank-3 guess (the exact solution has QTT rank 2)
+    A, _ = qtt_laplacian_1d(6)
+    b = tt.ones([2] * 6)
+    x0 = tt.ones([2] * 6, ranks=3).orthonormalize(canonical="right")
+    amen_case("als_qtt_lap1d_o6", A, b, x0, solver=als, residual_tol=1e-8, max_sweeps=10,
+              symmetric=True)
+    # 4-D Laplacian, rank-6 random guess, MINRES local solves
+    A = ref_train(P.laplacian_nd(4, 8))
+    b = tt.rand([8] * 4, ranks=2, seed=0)
+    x0 = tt.rand([8] * 4, ranks=6, seed=1)
+    amen_case("als_lap4_minres", A, b, x0, solver=als, residual_tol=1e-6, max_sweeps=6,
+              symmetric=True, direct_solve_size=100)
+    # non-symmetric, GMRES local solves, default guess (ranks of b)
+    rng = np.random.default_rng(5)
+    mat = np.eye(32) + 0.3 * rng.random((32, 32))
+    A = tt.tt_svd(mat.reshape([2] * 10), physical_indexes=[(2, 2)] * 5, ttm=True, error=0)
+    b = tt.tt_svd(rng.random(32).reshape([2] * 5), error=0)
+    amen_case("als_nonsym_gmres", A, b, solver=als, max_sweeps=4, direct_solve_size=4)
+
+
 def main() -> None:
+    if "als" in sys.argv[1:]:
+        als_cases()
+        return
     meta = {"reference_version": tt.__version__, "numpy": np.__version__}
     import scipy
     meta["scipy"] = scipy.__version__
@@ -209,6 +238,8 @@ def main() -> None:
     data["residual"] = np.array(relative_residual(A, b, x))
     data["b_norm"] = np.array(b.tt_norm())
     save("dot_residual", data, {})
+
+    als_cases()
 
     with open(os.path.join(HERE, "meta.json"), "w") as fh:
         json.dump(meta, fh, indent=1)

@@ -1,6 +1,6 @@
 """B200-native tensor-train solve path: AMEn, TT rounding, TTM-by-TT.
 
-Drop-in replacements for the reference entry points ``amen``,
+Drop-in replacements for the reference entry points ``amen``, ``als``,
 ``TensorTrain.truncate`` and ``TensorTrain.dot`` (ttnumpy 0.3.0), computed
 by hand-written sm_100a kernels in ``libttb200.so`` (C ABI in
 ``include/ttb200.h``).  There is no CPU path: the entry points raise when
@@ -16,6 +16,7 @@ from .solvers.common import (  # noqa: F401
     TruncationMode,
     relative_residual,
 )
+from .solvers.als import als  # noqa: F401
 from .solvers.amen import amen  # noqa: F401
 from .tensor_train import (  # noqa: F401
     DimensionMismatch,
@@ -30,7 +31,7 @@ from .tensor_train import (  # noqa: F401
 )
 
 __all__ = [
-    "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen",
+    "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen", "als",
     "SolverInfo", "StopReason", "LocalSolver", "TruncationMode", "relative_residual",
     "DimensionMismatch", "WrongTTFormat", "WrongTTType",
 ]
