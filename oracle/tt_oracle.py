@@ -300,9 +300,62 @@ def compress_svd(t: Train, error: float = 0.0, max_rank=None, canonical="auto") 
     return t
 
 
-def truncate(t: Train, error: float = 0.0, max_rank=None, canonical="auto") -> Train:
-    """TT rounding, ``method='direct'`` (``tensor_train.py:852-940``):
-    QR canonicalisation towards one end, then the SVD sweep back."""
+def sketch_rank(max_rank, options) -> int:
+    """Bond of the random sketch (``tensor_train.py:122-140``)."""
+    if max_rank is None:
+        raise ValueError("method='randomized' needs max_rank")
+    options = {} if options is None else options
+    if set(options) - {"oversampling"}:
+        raise ValueError("unknown options")
+    over = options.get("oversampling", 10)
+    if not isinstance(over, (int, np.integer)) or isinstance(over, bool) or over < 0:
+        raise ValueError("oversampling must be a non-negative integer")
+    return max_rank + over
+
+
+def randomized_left_orth(cores: List[np.ndarray], rank: int, rng) -> List[np.ndarray]:
+    """Randomize-then-orthogonalise, left to right
+    (``left_randomized_orthonormalize``, ``utils.py:139-203``): sketches of
+    the cores to the right of each bond against a Gaussian train (drawn
+    right to left, each sketch scaled by its largest entry), then the QR of
+    each unfolding times the next sketch."""
+    if rank < 1:
+        raise ValueError("rank must be positive")
+    count = len(cores)
+    sketches = [None] * count + [np.ones((1, 1))]
+    for i in range(count - 1, 0, -1):
+        contracted = _mul_right(cores[i], sketches[i + 1])
+        contracted = contracted.reshape(contracted.shape[0], -1)
+        bond = min(rank, *contracted.shape)
+        sk = contracted @ rng.standard_normal((contracted.shape[1], bond))
+        scale = np.abs(sk).max()
+        if scale > 0:
+            sk /= scale
+        sketches[i] = sk
+    for i in range(count - 1):
+        shape = cores[i].shape
+        matrix = cores[i].reshape(shape[0] * shape[1] * shape[2], shape[3])
+        q, _ = sla.qr(matrix @ sketches[i + 1], mode="economic")
+        cores[i] = q.reshape(shape[0], shape[1], shape[2], -1)
+        cores[i + 1] = _mul_left(q.T @ matrix, cores[i + 1])
+    return cores
+
+
+def randomized_right_orth(cores: List[np.ndarray], rank: int, rng) -> List[np.ndarray]:
+    """Mirror image of :func:`randomized_left_orth` (``utils.py:206-236``)."""
+    mirrored = [c.transpose(3, 1, 2, 0) for c in reversed(cores)]
+    mirrored = randomized_left_orth(mirrored, rank, rng)
+    cores[:] = [np.ascontiguousarray(c.transpose(3, 1, 2, 0)) for c in reversed(mirrored)]
+    return cores
+
+
+def truncate(t: Train, error: float = 0.0, max_rank=None, canonical="auto", method="direct",
+             seed=None, options=None) -> Train:
+    """TT rounding (``tensor_train.py:852-940``): QR (``method='direct'``)
+    or sketched (``'randomized'``) canonicalisation towards one end, then
+    the SVD sweep back."""
+    if method == "randomized":
+        rank = sketch_rank(max_rank, options)
     out = t.copy()
     orth_form = "left" if canonical == "right" else "right"
     if canonical == "auto":
@@ -310,7 +363,16 @@ def truncate(t: Train, error: float = 0.0, max_rank=None, canonical="auto") -> T
             orth_form = "left"
         else:
             orth_form = "right"
-    orthonormalize(out, orth_form)
+    if method == "direct":
+        orthonormalize(out, orth_form)
+    else:
+        rng = np.random.default_rng(seed)
+        if orth_form == "left":
+            randomized_left_orth(out.cores, rank, rng)
+            out.orth_center = len(out) - 1
+        else:
+            randomized_right_orth(out.cores, rank, rng)
+            out.orth_center = 0
     compress_svd(out, error, max_rank)
     return out
 

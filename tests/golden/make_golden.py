@@ -5,6 +5,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
 
     python tests/golden/make_golden.py          # every case
     python tests/golden/make_golden.py als      # the ALS cases only
+    python tests/golden/make_golden.py randomized  # randomized rounding only
 
 Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
 cores as ``<train>_<k>`` arrays plus ``<train>_n``), the call's arguments
@@ -122,9 +123,44 @@ def als_cases() -> None:
     amen_case("als_nonsym_gmres", A, b, solver=als, max_sweeps=4, direct_solve_size=4)
 
 
+def randomized_cases() -> None:
+    """truncate(method="randomized") (tensor_train.py:913-937 with
+    utils.py:139-236): the sketch-then-orthogonalise rounding."""
+    data = {}
+    g = np.random.default_rng(21)
+    cases = []
+    # a sum of two rank-6 Gaussian trains (true bonds <= 12), d = 7, n = 3
+    ranks = [1] + [6] * 6 + [1]
+    p = tt.TensorTrain([g.standard_normal((ranks[k], 3, 1, ranks[k + 1])) for k in range(7)])
+    q = tt.TensorTrain([g.standard_normal((ranks[k], 3, 1, ranks[k + 1])) for k in range(7)])
+    s = p + q
+    s.orth_center = None
+    pack(data, "s", s)
+    # exact sketch (max_rank + oversampling >= every bond), both directions,
+    # a lossy sketch (oversampling 0, max_rank below the true bonds) and a
+    # TTM train
+    for name, kw in [("left_exact", dict(max_rank=12, canonical="right", seed=4)),
+                     ("right_exact", dict(max_rank=12, canonical="left", seed=5)),
+                     ("auto_err", dict(max_rank=8, error=1e-2, seed=6)),
+                     ("lossy", dict(max_rank=5, seed=7, options={"oversampling": 0}))]:
+        out = s.truncate(method="randomized", **kw)
+        pack(data, f"out_{name}", out)
+        cases.append((name, kw))
+    A = tt.TensorTrain([g.standard_normal((ranks[k], 2, 3, ranks[k + 1])) for k in range(7)])
+    A.orth_center = None
+    pack(data, "A", A)
+    out = A.truncate(method="randomized", max_rank=4, seed=8, options={"oversampling": 3})
+    pack(data, "out_ttm", out)
+    cases.append(("ttm", dict(max_rank=4, seed=8, options={"oversampling": 3})))
+    save("truncate_randomized", data, {"cases": [[n, kw] for n, kw in cases]})
+
+
 def main() -> None:
     if "als" in sys.argv[1:]:
         als_cases()
+        return
+    if "randomized" in sys.argv[1:]:
+        randomized_cases()
         return
     meta = {"reference_version": tt.__version__, "numpy": np.__version__}
     import scipy
@@ -240,6 +276,7 @@ def main() -> None:
     save("dot_residual", data, {})
 
     als_cases()
+    randomized_cases()
 
     with open(os.path.join(HERE, "meta.json"), "w") as fh:
         json.dump(meta, fh, indent=1)

@@ -143,3 +143,47 @@ def test_round_batch_matches_oracle(tt, d, n, r, err, mr, gauss):
         got = otrain(res.train(i))
         assert got.bonds == want.bonds
         assert rel_tt(got, want) < max(1e-10, 0.01 * err)
+
+
+def test_randomized_truncate_matches_reference(tt):
+    """``truncate(method="randomized")`` against the reference's results:
+    the same Gaussian sketch (drawn on the host from the seed), QRs and SVD
+    sweep on the device; bonds, orthogonality centre and the rounded train
+    (TT difference, 1e-10 relative) agree, including a lossy sketch and a
+    TTM train."""
+    data = load_golden("truncate_randomized")
+    for name, kw in data["args"]["cases"]:
+        key = "A" if name == "ttm" else "s"
+        cores, oc = golden_train(data, key)
+        src = tt.TensorTrain(cores, orth_center=oc)
+        out = src.truncate(method="randomized", **kw)
+        ref_c, ref_oc = golden_train(data, f"out_{name}")
+        ref = O.Train(ref_c)
+        assert out.bonds == ref.bonds, name
+        assert out.orth_center == ref_oc, name
+        got = O.Train(out.to_numpy())
+        diff = O.tt_norm(O.add(got, O.scale(ref, -1.0))) / O.tt_norm(ref)
+        assert diff < 1e-10, (name, diff)
+
+
+def test_randomized_truncate_errors(tt):
+    t = tt.TensorTrain(P.random_tt([3] * 4, 3, seed=1))
+    with pytest.raises(ValueError):
+        t.truncate(method="randomized")  # needs max_rank
+    with pytest.raises(ValueError):
+        t.truncate(method="randomized", max_rank=2, options={"bogus": 1})
+    with pytest.raises(ValueError):
+        t.truncate(method="randomized", max_rank=2, options={"oversampling": -1})
+    with pytest.raises(ValueError):
+        t.truncate(method="sketch")
+
+
+def test_randomized_rounding_of_products(tt):
+    """``dot(..., truncate=True, method="randomized")`` rounds the product
+    exactly as ``truncate`` of the product does with the same seed."""
+    A = tt.TensorTrain(P.laplacian_nd(4, 5))
+    x = tt.TensorTrain(P.random_tt([5] * 4, 3, seed=2))
+    direct = A.dot(x).truncate(method="randomized", max_rank=4, seed=9)
+    fused = A.dot(x, truncate=True, max_rank=4, method="randomized", seed=9)
+    assert direct.bonds == fused.bonds
+    assert all(np.array_equal(u, v) for u, v in zip(direct.to_numpy(), fused.to_numpy()))

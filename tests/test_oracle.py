@@ -163,3 +163,17 @@ def test_problem_builders_dense():
                 if 0 <= q[ax] < n:
                     M[i, idx[tuple(q)]] -= c
     np.testing.assert_allclose(A.full(), M, rtol=1e-11, atol=1e-8)
+
+
+def test_oracle_randomized_truncate_matches_reference():
+    """``truncate(method="randomized")`` (``tensor_train.py:913-937``,
+    ``utils.py:139-236``): same Gaussian draws, same QRs and SVDs."""
+    data = load_golden("truncate_randomized")
+    for name, kw in data["args"]["cases"]:
+        src = _train(data, "A" if name == "ttm" else "s")
+        out = O.truncate(src, method="randomized", **kw)
+        ref = _train(data, f"out_{name}")
+        assert out.bonds == ref.bonds, name
+        diff = O.tt_norm(O.add(out, O.scale(ref, -1.0))) / O.tt_norm(ref)
+        assert diff <= 1e-12, (name, diff)
+        assert out.orth_center == ref.orth_center, name

@@ -211,7 +211,7 @@ class TensorTrain:
             descs.append(K.copy_desc(b, out[ranks[i] - rb[i]:, :, :, ranks[i + 1] - rb[i + 1]:]))
         K.copy_many(descs)
         res = TensorTrain._wrap(cores)
-        return _round_result(res, truncate, error, max_rank, method)
+        return _round_result(res, truncate, error, max_rank, method, seed, options)
 
     def __add__(self, other):
         return self.add(other)
@@ -224,7 +224,7 @@ class TensorTrain:
             res = self.copy()
             k = res.orth_center if res.orth_center is not None else 0
             K.copy_(res.cores[k], self.cores[k], float(other))
-            return _round_result(res, truncate, error, max_rank, method)
+            return _round_result(res, truncate, error, max_rank, method, seed, options)
         if isinstance(other, TensorTrain):
             raise NotImplementedError("element-wise products of two trains are not on the "
                                       "tensor-train solve path")
@@ -253,7 +253,8 @@ class TensorTrain:
             raise DimensionMismatch("Tensor trains must have the same last and first physical "
                                     "dimensions respectively")
         cores = [K.kron(a, x) for a, x in zip(self.cores, other.cores)]
-        return _round_result(TensorTrain._wrap(cores), truncate, error, max_rank, method)
+        return _round_result(TensorTrain._wrap(cores), truncate, error, max_rank, method, seed,
+                             options)
 
     def __matmul__(self, other):
         return self.dot(other)
@@ -352,7 +353,7 @@ class TensorTrain:
         if method not in ("direct", "randomized"):
             raise ValueError(f"Method must be 'direct' or 'randomized', but got {method!r}")
         if method == "randomized":
-            raise NotImplementedError("randomized rounding is not part of the solve path")
+            rank = _sketch_rank(max_rank, options)
         t = self if inplace else self.copy()
         orth_form = "left" if canonical == "right" else "right"
         if canonical == "auto":
@@ -360,7 +361,16 @@ class TensorTrain:
                 orth_form = "left"
             else:
                 orth_form = "right"
-        t.orthonormalize(canonical=orth_form, inplace=True)
+        if method == "direct":
+            t.orthonormalize(canonical=orth_form, inplace=True)
+        else:
+            rng = np.random.default_rng(seed)
+            if orth_form == "left":
+                randomized_left_orth(t.cores, rank, rng)
+                t.orth_center = len(t) - 1
+            else:
+                randomized_right_orth(t.cores, rank, rng)
+                t.orth_center = 0
         t.compress_svd(error, max_rank, inplace=True)
         return t
 
@@ -370,14 +380,14 @@ class TensorTrain:
                 f"{self.physical_dims()}")
 
 
-def _round_result(res, truncate, error, max_rank, method):
+def _round_result(res, truncate, error, max_rank, method, seed=None, options=None):
     """``_round_result`` (``tensor_train.py:94-119``)."""
     if not truncate:
         if method != "direct" or error is not None or max_rank is not None:
             raise ValueError("error, max_rank and method need truncate=True")
         return res
     return res.truncate(error=0.0 if error is None else error, max_rank=max_rank, inplace=True,
-                        method=method)
+                        method=method, seed=seed, options=options)
 
 
 # ---------------------------------------------------------------------------
@@ -399,6 +409,70 @@ def _apply_right(core: torch.Tensor, matrix: torch.Tensor) -> torch.Tensor:
                       device="cuda")
     K.gemm(core.reshape(-1, core.shape[-1]), matrix, out.view(-1, matrix.shape[1]))
     return out
+
+
+def _sketch_rank(max_rank: Optional[int], options: Optional[dict]) -> int:
+    """Bond of the random sketch of ``method="randomized"``
+    (``tensor_train.py:122-140``)."""
+    if max_rank is None:
+        raise ValueError("method='randomized' needs max_rank")
+    options = {} if options is None else options
+    unknown = set(options) - {"oversampling"}
+    if unknown:
+        raise ValueError(f"Unknown options for method='randomized': {sorted(unknown)}")
+    over = options.get("oversampling", 10)
+    if not isinstance(over, numbers.Integral) or isinstance(over, bool) or over < 0:
+        raise ValueError(f"oversampling must be a non-negative integer, but got {over!r}")
+    return max_rank + over
+
+
+def randomized_left_orth(cores: List[torch.Tensor], rank: int, rng) -> List[torch.Tensor]:
+    """Randomize-then-orthogonalise (``left_randomized_orthonormalize``,
+    ``utils.py:139-203``) on the device: the cores right of each bond are
+    contracted with a Gaussian train (its cores drawn on the host from
+    ``rng`` in the reference's order and shapes), then every unfolding
+    times the next sketch is factorised by QR and the remainder moved right.
+    Each sketch is scaled to unit norm (the reference scales by its largest
+    entry; a positive scale leaves the Q factors unchanged, it only keeps
+    long trains from overflowing)."""
+    if rank < 1:
+        raise ValueError(f"rank must be positive, but got {rank}")
+    count = len(cores)
+    sketches: List[Optional[torch.Tensor]] = [None] * count + [K.fill_(K.empty(1, 1), 1.0)]
+    nrm = K.empty(1)
+    for i in range(count - 1, 0, -1):
+        c = cores[i]
+        contracted = K.matmul(c.reshape(-1, c.shape[3]), sketches[i + 1])
+        cols = contracted.numel() // c.shape[0]
+        contracted = contracted.view(c.shape[0], cols)
+        bond = min(rank, c.shape[0], cols)
+        gauss = torch.from_numpy(rng.standard_normal((cols, bond))).to("cuda")
+        sk = K.matmul(contracted, gauss)
+        K.norm_into(nrm, sk)
+        scale = float(nrm.item())
+        if scale > 0:
+            K.copy_(sk, sk, alpha=1.0 / scale)
+        sketches[i] = sk
+    for i in range(count - 1):
+        s = cores[i].shape
+        matrix = cores[i].reshape(s[0] * s[1] * s[2], s[3])
+        q, _ = K.qr(K.matmul(matrix, sketches[i + 1]), want_r=False)
+        cores[i] = q.reshape(s[0], s[1], s[2], q.shape[1])
+        cores[i + 1] = _apply_left(K.matmul(q.t(), matrix), cores[i + 1])
+    return cores
+
+
+def randomized_right_orth(cores: List[torch.Tensor], rank: int, rng) -> List[torch.Tensor]:
+    """Mirror image of :func:`randomized_left_orth`
+    (``right_randomized_orthonormalize``, ``utils.py:206-236``)."""
+    def mirror(c):
+        out = K.empty(c.shape[3], c.shape[1], c.shape[2], c.shape[0])
+        return K.copy_(out, c.permute(3, 1, 2, 0))
+
+    mirrored = [mirror(c) for c in reversed(cores)]
+    randomized_left_orth(mirrored, rank, rng)
+    cores[:] = [mirror(c) for c in reversed(mirrored)]
+    return cores
 
 
 def left_orth_sweep(cores: List[torch.Tensor], start: int, end: int) -> None:
