@@ -882,3 +882,44 @@ def als(A: Train, b: Train, x0: Optional[Train] = None, max_sweeps=4, residual_t
                 info.stop_reason = "stagnated"
                 break
     return x, info
+
+
+def tt_svd(tensor: np.ndarray, error: float = 1e-12, max_rank=None, physical_indexes=None,
+           ttm: bool = False) -> Train:
+    """TT-SVD (``tensor_train.py:1138-1247``): left to right, the unfolding
+    (bond * modes_i, rest) is split by an SVD (gesvd), truncated with
+    ``truncated_bond`` at ``delta = error / sqrt(ndim - 1) * ||tensor||``
+    and the remainder ``U^T @ matrix`` carried on."""
+    t = np.array(tensor, dtype=np.float64, copy=True)
+    if t.ndim == 1 and physical_indexes is None:
+        raise ValueError("1-D tensor needs physical_indexes")
+    if physical_indexes is not None:
+        if ttm:
+            d = len(physical_indexes)
+            perm = tuple(np.arange(2 * d).reshape(2, d).T.flatten())
+            t = np.transpose(t, perm).reshape([x for pair in physical_indexes for x in pair])
+            phys = [tuple(p) for p in physical_indexes]
+        else:
+            t = t.reshape(physical_indexes)
+            phys = [(x, 1) for x in physical_indexes]
+    else:
+        if ttm:
+            raise ValueError("TTM needs physical_indexes")
+        phys = [(x, 1) for x in t.shape]
+    norm = float(np.linalg.norm(t))
+    delta = error / np.sqrt(t.ndim - 1) * norm
+    cores, bond = [], 1
+    for i in range(len(phys) - 1):
+        rest = int(np.prod([int(np.prod(p)) for p in phys[i + 1:]]))
+        matrix = t.reshape(bond * int(np.prod(phys[i])), rest)
+        u, s, _ = sla.svd(matrix, full_matrices=False, check_finite=False, lapack_driver="gesvd")
+        nb = truncated_bond(s, delta, max_rank)
+        ut = u[:, :nb]
+        cores.append(ut.reshape((bond,) + tuple(phys[i]) + (nb,)))
+        c = ut.T @ matrix
+        if i == len(phys) - 2:
+            cores.append(c.reshape((c.shape[0],) + tuple(phys[i + 1]) + (1,)))
+        else:
+            bond = c.shape[0]
+            t = c
+    return Train(cores, orth_center=len(cores) - 1)

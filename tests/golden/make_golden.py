@@ -6,6 +6,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
     python tests/golden/make_golden.py          # every case
     python tests/golden/make_golden.py als      # the ALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
+    python tests/golden/make_golden.py tt_svd   # TT-SVD only
 
 Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
 cores as ``<train>_<k>`` arrays plus ``<train>_n``), the call's arguments
@@ -155,7 +156,38 @@ def randomized_cases() -> None:
     save("truncate_randomized", data, {"cases": [[n, kw] for n, kw in cases]})
 
 
+def tt_svd_cases() -> None:
+    """tt_svd (tensor_train.py:1138-1247): the dense-to-TT builder."""
+    data = {}
+    g = np.random.default_rng(31)
+    cases = []
+    # a rank-3 5-D tensor plus small noise, default and loose errors
+    f = sum(np.einsum("i,j,k,l,m->ijklm", *[g.standard_normal(n) for n in (4, 5, 3, 6, 4)])
+            for _ in range(3)) + 1e-6 * g.standard_normal((4, 5, 3, 6, 4))
+    data["dense"] = f
+    for name, kw in [("default", {}), ("loose", {"error": 1e-3}), ("cap", {"max_rank": 2})]:
+        pack(data, f"out_{name}", tt.tt_svd(f, **kw))
+        cases.append([name, "dense", kw])
+    # the QTT of sin(pi x) sin(pi y) on a 2^6 x 2^6 grid (physical indexes)
+    x = np.arange(1, 65) / 65.0
+    q = np.outer(np.sin(np.pi * x), np.sin(np.pi * x)).reshape(-1)
+    data["qtt_vec"] = q
+    pack(data, "out_qtt", tt.tt_svd(q, physical_indexes=[2] * 12, error=1e-12))
+    cases.append(["qtt", "qtt_vec", {"physical_indexes": [2] * 12, "error": 1e-12}])
+    # a TTM from a dense 16 x 16 matrix, pairs (2, 2) x 4
+    m = np.eye(16) + 0.1 * g.standard_normal((16, 16))
+    data["ttm_mat"] = m.reshape([2] * 8)
+    pack(data, "out_ttm", tt.tt_svd(m.reshape([2] * 8), physical_indexes=[(2, 2)] * 4,
+                                    ttm=True, error=1e-10))
+    cases.append(["ttm", "ttm_mat", {"physical_indexes": [[2, 2]] * 4, "ttm": True,
+                                     "error": 1e-10}])
+    save("tt_svd", data, {"cases": cases})
+
+
 def main() -> None:
+    if "tt_svd" in sys.argv[1:]:
+        tt_svd_cases()
+        return
     if "als" in sys.argv[1:]:
         als_cases()
         return
@@ -277,6 +309,7 @@ def main() -> None:
 
     als_cases()
     randomized_cases()
+    tt_svd_cases()
 
     with open(os.path.join(HERE, "meta.json"), "w") as fh:
         json.dump(meta, fh, indent=1)

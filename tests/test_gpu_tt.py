@@ -187,3 +187,30 @@ def test_randomized_rounding_of_products(tt):
     fused = A.dot(x, truncate=True, max_rank=4, method="randomized", seed=9)
     assert direct.bonds == fused.bonds
     assert all(np.array_equal(u, v) for u, v in zip(direct.to_numpy(), fused.to_numpy()))
+
+
+def test_tt_svd_matches_reference(tt):
+    """``tt_svd`` on the device against the reference's trains: the same
+    bonds and centre, and the same tensor (dense comparison; the SVD signs
+    may differ, the product may not)."""
+    data = load_golden("tt_svd")
+    for name, src, kw in data["args"]["cases"]:
+        kw = dict(kw)
+        if "physical_indexes" in kw:
+            kw["physical_indexes"] = [tuple(p) if isinstance(p, list) else p
+                                      for p in kw["physical_indexes"]]
+        dense = np.asarray(data[src])
+        for inp in (dense, torch.from_numpy(dense).cuda()):
+            out = tt.tt_svd(inp, **kw)
+            ref_c, ref_oc = golden_train(data, f"out_{name}")
+            assert out.bonds == O.Train(ref_c).bonds, name
+            assert out.orth_center == ref_oc
+            got, want = O.Train(out.to_numpy()).full(), O.Train(ref_c).full()
+            assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want), name
+
+
+def test_tt_svd_errors(tt):
+    with pytest.raises(tt.AmbiguousFormat):
+        tt.tt_svd(np.ones(8))
+    with pytest.raises(tt.AmbiguousFormat):
+        tt.tt_svd(np.ones((2, 2)), ttm=True)

@@ -177,3 +177,19 @@ def test_oracle_randomized_truncate_matches_reference():
         diff = O.tt_norm(O.add(out, O.scale(ref, -1.0))) / O.tt_norm(ref)
         assert diff <= 1e-12, (name, diff)
         assert out.orth_center == ref.orth_center, name
+
+
+def test_oracle_tt_svd_matches_reference():
+    """``tt_svd`` (``tensor_train.py:1138-1247``): same bonds, same train
+    (the same LAPACK gesvd, so the same signs) and the same centre."""
+    data = load_golden("tt_svd")
+    for name, src, kw in data["args"]["cases"]:
+        kw = dict(kw)
+        if "physical_indexes" in kw:
+            kw["physical_indexes"] = [tuple(p) if isinstance(p, list) else p
+                                      for p in kw["physical_indexes"]]
+        out = O.tt_svd(data[src], **kw)
+        ref = _train(data, f"out_{name}")
+        assert out.bonds == ref.bonds, name
+        assert all(np.allclose(a, b, rtol=1e-10, atol=1e-12) for a, b in zip(out.cores, ref.cores)), name
+        assert out.orth_center == ref.orth_center == len(ref) - 1

@@ -19,6 +19,7 @@ from .solvers.common import (  # noqa: F401
 from .solvers.als import als  # noqa: F401
 from .solvers.amen import amen  # noqa: F401
 from .tensor_train import (  # noqa: F401
+    AmbiguousFormat,
     DimensionMismatch,
     TensorTrain,
     TensorTrainType,
@@ -27,11 +28,12 @@ from .tensor_train import (  # noqa: F401
     eye,
     ones,
     rand,
+    tt_svd,
     zeros,
 )
 
 __all__ = [
     "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen", "als",
     "SolverInfo", "StopReason", "LocalSolver", "TruncationMode", "relative_residual",
-    "DimensionMismatch", "WrongTTFormat", "WrongTTType",
+    "DimensionMismatch", "WrongTTFormat", "WrongTTType", "AmbiguousFormat", "tt_svd",
 ]

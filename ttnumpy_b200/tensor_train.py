@@ -25,6 +25,14 @@ from . import kernels as K
 logger = logging.getLogger("ttnumpy")
 
 
+class AmbiguousFormat(Exception):
+    """Not enough information to define a train (``tensor_train.py:45-50``)."""
+
+    def __init__(self, msg="Not enough information to define object"):
+        self.msg = msg
+        super().__init__(self.msg)
+
+
 class DimensionMismatch(Exception):
     """Exception for dimension errors (``tensor_train.py:21-26``)."""
 
@@ -534,6 +542,67 @@ def right_svd_sweep(cores: List[torch.Tensor], error: float, max_rank=None) -> N
         K.copy_(carry, u[:, :nb], scale=sv, scale_axis=1)
         cores[i] = core
         cores[i - 1] = _apply_right(cores[i - 1], carry)
+
+
+# ---------------------------------------------------------------------------
+# TT-SVD (tensor_train.py:1138-1247) on the device
+# ---------------------------------------------------------------------------
+
+
+def tt_svd(tensor, error: float = 1e-12, max_rank: Optional[int] = None,
+           physical_indexes=None, ttm: bool = False) -> TensorTrain:
+    """Dense tensor (numpy array or CUDA tensor) to a train by TT-SVD, as
+    the reference's ``tt_svd`` (``tensor_train.py:1138-1247``): each
+    unfolding (bond * modes_i, rest) is split by a device SVD, truncated by
+    the tail-norm rule at ``delta = error / sqrt(ndim - 1) * ||tensor||``
+    and ``U^T @ matrix`` carried to the next split.  A tensor already on the
+    GPU stays there (a TTM's index pairs are interleaved by one transposing
+    copy).  The result is left-orthonormal with its centre on the last core.
+    """
+    if isinstance(tensor, torch.Tensor):
+        t = tensor.to(device="cuda", dtype=torch.float64)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(tensor, dtype=np.float64)).to("cuda")
+    if t.dim() == 1 and physical_indexes is None:
+        raise AmbiguousFormat("For 1 dimensional tensor physical indexes need to be provided")
+    if max_rank is not None and max_rank <= 0:
+        raise ValueError("max_rank must be a positive integer.")
+    if physical_indexes is not None:
+        if ttm:
+            d = len(physical_indexes)
+            perm = tuple(int(v) for v in np.arange(2 * d).reshape(2, d).T.flatten())
+            t = t.permute(*perm).contiguous()
+            phys = [tuple(int(x) for x in pair) for pair in physical_indexes]
+            t = t.reshape([x for pair in phys for x in pair])
+        else:
+            phys = [(int(x), 1) for x in physical_indexes]
+            t = t.reshape([p[0] for p in phys])
+    else:
+        if ttm:
+            raise AmbiguousFormat("For Tensor Train Matrix type physical indexes is needed")
+        phys = [(int(x), 1) for x in t.shape]
+    t = t.contiguous()
+    nrm = K.empty(1)
+    K.norm_into(nrm, t.reshape(-1))
+    delta = error / math.sqrt(t.dim() - 1) * float(nrm.item()) if t.dim() > 1 else 0.0
+    if len(phys) == 1:
+        return TensorTrain._wrap([t.reshape((1,) + phys[0] + (1,))], orth_center=0)
+    cores: List[torch.Tensor] = []
+    bond, cur = 1, t.reshape(-1)
+    for i in range(len(phys) - 1):
+        rows = bond * phys[i][0] * phys[i][1]
+        matrix = cur.view(rows, -1)
+        u, sv, _ = K.svd(matrix)
+        nb = _svd_rank(sv, delta, max_rank)
+        core = K.empty(rows, nb)
+        K.copy_(core, u[:, :nb])
+        cores.append(core.view((bond,) + phys[i] + (nb,)))
+        c = K.matmul(core.t(), matrix)
+        if i == len(phys) - 2:
+            cores.append(c.view((nb,) + phys[i + 1] + (1,)))
+        else:
+            bond, cur = nb, c.reshape(-1)
+    return TensorTrain._wrap(cores, orth_center=len(cores) - 1)
 
 
 # ---------------------------------------------------------------------------
