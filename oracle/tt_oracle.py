@@ -923,3 +923,98 @@ def tt_svd(tensor: np.ndarray, error: float = 1e-12, max_rank=None, physical_ind
             bond = c.shape[0]
             t = c
     return Train(cores, orth_center=len(cores) - 1)
+
+
+def tt_to_qtt(t: Train, mode_size: int = 2, error: float = 1e-12, max_rank=None) -> Train:
+    """Quantisation of every mode (``tensor_train.py:942-1066``): after a
+    right QR sweep, each core of mode ``mode_size^q`` is split left to right
+    into q cores by q - 1 truncated SVDs (row and column halves kept
+    paired), and the remainder of each group is pushed into the next core
+    by one more SVD; one error budget ``error / sqrt(#SVDs) * ||t||``."""
+    if mode_size < 2:
+        raise ValueError("mode_size must be at least 2")
+    if max_rank is not None and max_rank <= 0:
+        raise ValueError("max_rank must be a positive integer.")
+    nums = []
+    for i, m in enumerate(t.row_modes):
+        q = 0
+        while mode_size ** q < m:
+            q += 1
+        if mode_size ** q != m:
+            raise ValueError(f"Row mode {m} not a power of {mode_size}")
+        if t.is_ttm() and mode_size ** q != t.col_modes[i]:
+            raise ValueError("Column mode size of TTM not a power of mode size")
+        nums.append(q)
+    rms = mode_size
+    cms = mode_size if t.is_ttm() else 1
+    count = max(1, sum(max(0, q - 1) for q in nums) + len(t) - 1)
+    tt = orthonormalize(t.copy(), "right")
+    delta = error / np.sqrt(count) * tt_norm(tt)
+    out = []
+    for i, q in enumerate(nums):
+        core = tt.cores[i]
+        lb, rb = core.shape[0], core.shape[-1]
+        for j in range(q - 1, 0, -1):
+            core = core.reshape(lb, rms, rms ** j, cms, cms ** j, rb).transpose(0, 1, 3, 2, 4, 5)
+            matrix = core.reshape(lb * rms * cms, rms ** j * cms ** j * rb)
+            u, s, _ = sla.svd(matrix, full_matrices=False, check_finite=False, lapack_driver="gesvd")
+            nb = truncated_bond(s, delta, max_rank)
+            out.append(u[:, :nb].reshape(lb, rms, cms, nb))
+            core = u[:, :nb].T @ matrix
+            lb = nb
+        if i < len(t) - 1:
+            matrix = core.reshape(lb * rms * cms, rb)
+            u, s, _ = sla.svd(matrix, full_matrices=False, check_finite=False, lapack_driver="gesvd")
+            nb = truncated_bond(s, delta, max_rank)
+            out.append(u[:, :nb].reshape(lb, rms, cms, nb))
+            tt.cores[i + 1] = np.tensordot(u[:, :nb].T @ matrix, tt.cores[i + 1], axes=(1, 0))
+        else:
+            out.append(core.reshape(lb, rms, cms, rb))
+    return Train(out, orth_center=len(out) - 1)
+
+
+def merge_cores(cores: List[np.ndarray]) -> np.ndarray:
+    """Product of consecutive cores as one core (``tensor_train.py:57-92``,
+    ``_contract_cores`` and ``_merge_cores``): contract the bonds left to
+    right, then gather the row modes in front of the column modes."""
+    lb, rb = cores[0].shape[0], cores[-1].shape[-1]
+    rows = [c.shape[1] for c in cores]
+    cols = [c.shape[2] for c in cores]
+    m = cores[0].reshape(-1, cores[0].shape[-1])
+    for c in cores[1:]:
+        m = (m @ c.reshape(c.shape[0], -1)).reshape(-1, c.shape[-1])
+    # axes of size 1 are left out of the transpose (a group of many such
+    # cores would exceed NumPy's axis limit otherwise)
+    axes = [(k % 2, x) for k, x in enumerate(v for pair in zip(rows, cols) for v in pair) if x > 1]
+    inter = m.reshape([lb] + [x for _, x in axes] + [rb])
+    perm = ([0] + [1 + k for k, (kind, _) in enumerate(axes) if kind == 0]
+            + [1 + k for k, (kind, _) in enumerate(axes) if kind == 1] + [len(axes) + 1])
+    return inter.transpose(perm).reshape(lb, int(np.prod(rows)), int(np.prod(cols)), rb)
+
+
+def qtt_to_tt(t: Train, physical_indexes, error: float = 1e-12, max_rank=None) -> Train:
+    """Inverse quantisation (``tensor_train.py:1072-1135``): consecutive
+    cores are grouped so that each group's row (and, for a TTM, column)
+    modes multiply to the requested index, each group is merged into one
+    core, and the result is rounded by ``truncate``."""
+    ttm = t.is_ttm()
+    groups = []
+    pos = 0
+    for i, idx in enumerate(physical_indexes):
+        rt, ct = (idx if ttm else (idx, 1))
+        pr = pc = 1
+        n = 0
+        while n == 0 or pr != rt or pc != ct:
+            if pos + n >= len(t):
+                raise ValueError(f"Not enough QTT cores to match physical index for core {i}")
+            pr *= t.row_modes[pos + n]
+            pc *= t.col_modes[pos + n]
+            n += 1
+            if pr > rt or pc > ct:
+                raise ValueError(f"QTT mode size exceeds the original mode size for core {i}")
+        groups.append((pos, n))
+        pos += n
+    if pos != len(t):
+        raise ValueError(f"Physical indexes cover only {pos} of {len(t)} QTT cores")
+    merged = Train([merge_cores(t.cores[p:p + n]) for p, n in groups])
+    return truncate(merged, error=error, max_rank=max_rank)

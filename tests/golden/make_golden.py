@@ -7,6 +7,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
     python tests/golden/make_golden.py als      # the ALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
     python tests/golden/make_golden.py tt_svd   # TT-SVD only
+    python tests/golden/make_golden.py tt_to_qtt  # quantisation only
 
 Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
 cores as ``<train>_<k>`` arrays plus ``<train>_n``), the call's arguments
@@ -184,7 +185,51 @@ def tt_svd_cases() -> None:
     save("tt_svd", data, {"cases": cases})
 
 
+def tt_to_qtt_cases() -> None:
+    """TensorTrain.tt_to_qtt (tensor_train.py:942-1066) and its inverse
+    qtt_to_tt (tensor_train.py:1072-1135)."""
+    data = {}
+    g = np.random.default_rng(41)
+    cases = []
+    t = tt.rand([8, 16, 4, 2], ranks=3, seed=12)
+    pack(data, "t", t)
+    for name, kw in [("default", {}), ("loose", {"error": 1e-2}), ("cap", {"max_rank": 2})]:
+        pack(data, f"out_{name}", t.tt_to_qtt(**kw))
+        cases.append([name, "t", kw])
+    ranks = [1, 2, 3, 1]
+    A = tt.TensorTrain([g.standard_normal((ranks[k], m, m, ranks[k + 1]))
+                        for k, m in enumerate([4, 8, 4])])
+    pack(data, "A", A)
+    pack(data, "out_ttm", A.tt_to_qtt(error=1e-10))
+    cases.append(["ttm", "A", {"error": 1e-10}])
+    t9 = tt.rand([9, 3, 27], ranks=2, seed=13)
+    pack(data, "t9", t9)
+    pack(data, "out_base3", t9.tt_to_qtt(mode_size=3))
+    cases.append(["base3", "t9", {"mode_size": 3}])
+    # TensorTrain.qtt_to_tt (tensor_train.py:1072-1135) on the quantised trains
+    back = []
+    for name, src, idx in [
+        ("tt", "out_default", [8, 16, 4, 2]),
+        ("regroup", "out_default", [128, 4, 2]),
+        ("singles", "out_loose", [2] * 10),
+        ("ttm", "out_ttm", [(4, 4), (8, 8), (4, 4)]),
+        ("ttm_regroup", "out_ttm", [(32, 32), (4, 4)]),
+        ("base3", "out_base3", [9, 3, 27]),
+    ]:
+        q = tt.TensorTrain([data[f"{src}_{k}"] for k in range(int(data[f"{src}_n"]))])
+        pack(data, f"back_{name}", q.qtt_to_tt(idx, error=1e-12))
+        back.append([name, src, idx, {"error": 1e-12}])
+    ones = tt.rand([2] * 10 + [1] * 30 + [2] * 3, ranks=3, seed=7)
+    pack(data, "ones", ones)
+    pack(data, "back_ones", ones.qtt_to_tt([1024, 8]))
+    back.append(["ones", "ones", [1024, 8], {}])
+    save("tt_to_qtt", data, {"cases": cases, "back": back})
+
+
 def main() -> None:
+    if "tt_to_qtt" in sys.argv[1:]:
+        tt_to_qtt_cases()
+        return
     if "tt_svd" in sys.argv[1:]:
         tt_svd_cases()
         return
@@ -310,6 +355,7 @@ def main() -> None:
     als_cases()
     randomized_cases()
     tt_svd_cases()
+    tt_to_qtt_cases()
 
     with open(os.path.join(HERE, "meta.json"), "w") as fh:
         json.dump(meta, fh, indent=1)

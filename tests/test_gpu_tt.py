@@ -214,3 +214,84 @@ def test_tt_svd_errors(tt):
         tt.tt_svd(np.ones(8))
     with pytest.raises(tt.AmbiguousFormat):
         tt.tt_svd(np.ones((2, 2)), ttm=True)
+
+
+def _dense_close(out_cores, ref_cores, rel=1e-10):
+    got, want = O.Train(out_cores).full(), O.Train(ref_cores).full()
+    return np.linalg.norm(got - want) <= rel * np.linalg.norm(want)
+
+
+def test_tt_to_qtt_matches_reference(tt):
+    """``tt_to_qtt`` on the device against the reference's quantised trains
+    (``tensor_train.py:942-1066``): same bonds, modes and centre, the same
+    tensor, left-orthonormal cores, and the source left untouched."""
+    data = load_golden("tt_to_qtt")
+    for name, src, kw in data["args"]["cases"]:
+        src_c, _ = golden_train(data, src)
+        ref_c, ref_oc = golden_train(data, f"out_{name}")
+        t = tt.TensorTrain(src_c)
+        out = t.tt_to_qtt(**kw)
+        assert out.bonds == O.Train(ref_c).bonds, name
+        assert out.orth_center == ref_oc == len(ref_c) - 1, name
+        assert out.physical_dims() == [(c.shape[1], c.shape[2]) if c.shape[2] > 1 else c.shape[1]
+                                       for c in ref_c], name
+        cores = out.to_numpy()
+        assert _dense_close(cores, ref_c), name
+        for c in cores[:-1]:
+            m = c.reshape(-1, c.shape[-1])
+            assert np.allclose(m.T @ m, np.eye(m.shape[1]), atol=1e-12), name
+        assert all(np.array_equal(a, b) for a, b in zip(src_c, t.to_numpy())), name
+        assert t.orth_center is None
+
+
+def test_qtt_to_tt_matches_reference(tt):
+    """``qtt_to_tt`` on the device (``tensor_train.py:1072-1135``):
+    regroupings, TTM pairs and a 40-core group mostly of mode 1 against the
+    reference's merged and rounded trains."""
+    data = load_golden("tt_to_qtt")
+    for name, src, idx, kw in data["args"]["back"]:
+        idx = [tuple(p) if isinstance(p, list) else p for p in idx]
+        src_c, _ = golden_train(data, src)
+        ref_c, ref_oc = golden_train(data, f"back_{name}")
+        out = tt.TensorTrain(src_c).qtt_to_tt(idx, **kw)
+        assert out.bonds == O.Train(ref_c).bonds, name
+        assert out.orth_center == ref_oc, name
+        assert out.physical_dims() == idx, name
+        assert _dense_close(out.to_numpy(), ref_c), name
+
+
+def test_qtt_cycles_and_error_bound(tt):
+    """Five quantise/merge cycles keep the tensor; the quantisation error
+    stays within ``error * ||A||`` (reference tests/test_tensor_train.py:
+    458-481)."""
+    t = tt.rand([8] * 4, ranks=8, seed=118)
+    want = O.Train(t.to_numpy()).full()
+    for _ in range(5):
+        t = t.tt_to_qtt(error=1e-12).qtt_to_tt([8] * 4, error=1e-12)
+    assert np.linalg.norm(O.Train(t.to_numpy()).full() - want) <= 1e-10 * np.linalg.norm(want)
+    dense = np.random.default_rng(0).standard_normal((8, 8, 8))
+    src = tt.tt_svd(dense)
+    for err in (3e-1, 1e-1, 1e-2, 1e-4):
+        q = src.tt_to_qtt(error=err)
+        got = O.Train(q.to_numpy()).full().reshape(8, 8, 8)
+        assert np.linalg.norm(got - dense) <= err * np.linalg.norm(dense)
+    assert tt.rand([16, 16], ranks=4, seed=120).tt_to_qtt(error=1e2).bonds == [1] * 9
+
+
+def test_qtt_errors(tt):
+    t = tt.rand([4, 4], ranks=2, seed=123)
+    with pytest.raises(ValueError):
+        t.tt_to_qtt(max_rank=0)
+    with pytest.raises(ValueError):
+        t.tt_to_qtt(mode_size=1)
+    with pytest.raises(tt.DimensionMismatch):
+        t.tt_to_qtt(mode_size=3)
+    with pytest.raises(tt.DimensionMismatch):
+        tt.rand([(4, 2), (4, 2)], ranks=2, seed=124).tt_to_qtt()
+    q = tt.rand([4, 4, 4], ranks=3, seed=125).tt_to_qtt(error=1e-12)
+    for bad in ([4, 4], [8, 8, 8], [3, 8, 8]):
+        with pytest.raises(tt.DimensionMismatch):
+            q.qtt_to_tt(bad)
+    qm = tt.rand([(4, 4), (4, 4)], ranks=3, seed=126).tt_to_qtt(error=1e-12)
+    with pytest.raises(tt.DimensionMismatch):
+        qm.qtt_to_tt([(4, 2), (4, 8)])

@@ -193,3 +193,43 @@ def test_oracle_tt_svd_matches_reference():
         assert out.bonds == ref.bonds, name
         assert all(np.allclose(a, b, rtol=1e-10, atol=1e-12) for a, b in zip(out.cores, ref.cores)), name
         assert out.orth_center == ref.orth_center == len(ref) - 1
+
+
+def test_oracle_tt_to_qtt_matches_reference():
+    """``tt_to_qtt`` (``tensor_train.py:942-1066``): same bonds, same cores
+    (same LAPACK calls), centre on the last core."""
+    data = load_golden("tt_to_qtt")
+    for name, src, kw in data["args"]["cases"]:
+        out = O.tt_to_qtt(_train(data, src), **kw)
+        ref = _train(data, f"out_{name}")
+        assert out.bonds == ref.bonds, name
+        assert all(np.allclose(a, b, rtol=1e-9, atol=1e-12) for a, b in zip(out.cores, ref.cores)), name
+        assert out.orth_center == ref.orth_center == len(ref) - 1
+
+
+def test_oracle_qtt_to_tt_matches_reference():
+    """``qtt_to_tt`` (``tensor_train.py:1072-1135``): regroupings of the
+    quantised trains of the fixture, TTM pairs and a group of 40 cores most
+    of mode 1; same bonds and cores as the reference."""
+    data = load_golden("tt_to_qtt")
+    for name, src, idx, kw in data["args"]["back"]:
+        idx = [tuple(p) if isinstance(p, list) else p for p in idx]
+        out = O.qtt_to_tt(_train(data, src), idx, **kw)
+        ref = _train(data, f"back_{name}")
+        assert out.bonds == ref.bonds, name
+        assert all(np.allclose(a, b, rtol=1e-9, atol=1e-12) for a, b in zip(out.cores, ref.cores)), name
+        assert out.orth_center == ref.orth_center
+
+
+def test_oracle_qtt_round_trip_and_errors():
+    """Quantise and merge back returns the train; mismatched indexes raise
+    (``tests/test_tensor_train.py:592-620`` of the reference)."""
+    t = O.Train([np.random.default_rng(3).standard_normal(s) for s in
+                 [(1, 4, 1, 3), (3, 4, 1, 3), (3, 4, 1, 1)]])
+    q = O.tt_to_qtt(t, error=1e-13)
+    assert [c.shape[1] for c in q.cores] == [2] * 6
+    back = O.qtt_to_tt(q, [4, 4, 4], error=1e-13)
+    assert np.allclose(back.full(), t.full(), rtol=1e-11, atol=1e-12)
+    for bad in ([4, 4], [8, 8, 8], [3, 8, 8]):
+        with pytest.raises(ValueError):
+            O.qtt_to_tt(q, bad)

@@ -382,6 +382,109 @@ class TensorTrain:
         t.compress_svd(error, max_rank, inplace=True)
         return t
 
+    def tt_to_qtt(self, mode_size: int = 2, error: float = 1e-12,
+                  max_rank: Optional[int] = None) -> "TensorTrain":
+        """Quantise every mode into cores of mode ``mode_size``, as the
+        reference's ``tt_to_qtt`` (``tensor_train.py:942-1066``).
+
+        After a right QR sweep, a core of mode ``mode_size^q`` is split left
+        to right by q - 1 device SVDs of its (bond * mode_size, rest)
+        unfolding (a TTM's row and column halves kept paired by one strided
+        copy per split), and the remainder of each group is pushed into the
+        next core by one more SVD.  Every split truncates at
+        ``delta = error / sqrt(#SVDs) * ||t||``.  The result is
+        left-orthonormal with its centre on the last core.
+        """
+        if mode_size < 2:
+            raise ValueError(f"mode_size must be at least 2, but got {mode_size}")
+        if max_rank is not None and max_rank <= 0:
+            raise ValueError("max_rank must be a positive integer.")
+        ttm = self.is_ttm()
+        nums = []
+        for i, m in enumerate(self.row_modes):
+            q = 0
+            while mode_size ** q < m:
+                q += 1
+            if mode_size ** q != m:
+                raise DimensionMismatch(f"Row mode {m} not a power of {mode_size}")
+            if ttm and mode_size ** q != self.col_modes[i]:
+                raise DimensionMismatch("Column mode size of TTM not a power of mode size")
+            if q == 0:
+                raise ValueError("a core of mode 1 cannot be split into cores of mode "
+                                 f"{mode_size}")
+            nums.append(q)
+        rms, cms = mode_size, (mode_size if ttm else 1)
+        count = max(1, sum(q - 1 for q in nums) + len(self) - 1)
+        t = self.orthonormalize(canonical="right")
+        delta = error / math.sqrt(count) * t.tt_norm()
+        cores = t.cores
+        out: List[torch.Tensor] = []
+
+        def split(matrix: torch.Tensor, lb: int):
+            u, sv, _ = K.svd(matrix)
+            nb = _svd_rank(sv, delta, max_rank)
+            piece = K.empty(matrix.shape[0], nb)
+            K.copy_(piece, u[:, :nb])
+            out.append(piece.view(lb, rms, cms, nb))
+            return K.matmul(piece.t(), matrix), nb
+
+        for i, q in enumerate(nums):
+            core = cores[i].reshape(-1)  # laid out (lb, rms, rms^j, cms, cms^j, rb)
+            lb, rb = cores[i].shape[0], cores[i].shape[-1]
+            for j in range(q - 1, 0, -1):
+                tail = cms ** j * rb
+                if cms > 1:  # bring the first column factor next to the first row factor
+                    matrix = K.empty(lb * rms * cms, rms ** j * tail)
+                    K.copy_(matrix.view(lb * rms, cms, rms ** j, tail),
+                            core.as_strided((lb * rms, cms, rms ** j, tail),
+                                            (rms ** j * cms * tail, tail, cms * tail, 1)))
+                else:
+                    matrix = core.view(lb * rms, -1)
+                core, lb = split(matrix, lb)
+                core = core.reshape(-1)
+            if i < len(nums) - 1:
+                carry, _ = split(core.view(lb * rms * cms, rb), lb)
+                cores[i + 1] = _apply_left(carry, cores[i + 1])
+            else:
+                out.append(core.view(lb, rms, cms, rb))
+        return TensorTrain._wrap(out, orth_center=len(out) - 1)
+
+    def qtt_to_tt(self, physical_indexes, error: float = 1e-12,
+                  max_rank: Optional[int] = None) -> "TensorTrain":
+        """Merge groups of consecutive quantised cores back into one core
+        each and round the result, as the reference's ``qtt_to_tt``
+        (``tensor_train.py:1072-1135``): a group takes cores until its row
+        (and, for a TTM, column) modes multiply to the requested index.
+        Merging is one device GEMM per core plus, for a TTM, one strided
+        copy that moves the new row factor in front of the column factors.
+        """
+        ttm = self.is_ttm()
+        groups = []
+        pos = 0
+        for i, idx in enumerate(physical_indexes):
+            rt, ct = (idx if ttm else (idx, 1))
+            pr = pc = 1
+            n = 0
+            while n == 0 or pr != rt or pc != ct:
+                if pos + n >= len(self):
+                    raise DimensionMismatch(
+                        f"Not enough QTT cores to match physical index for core {i}")
+                pr *= self.row_modes[pos + n]
+                pc *= self.col_modes[pos + n]
+                n += 1
+                if pr > rt:
+                    raise DimensionMismatch(
+                        f"Row mode size of QTT exceeds original row mode size for core {i}")
+                if pc > ct:
+                    raise DimensionMismatch(
+                        f"Column mode size of QTT exceeds original column mode size for core {i}")
+            groups.append((pos, n))
+            pos += n
+        if pos != len(self):
+            raise DimensionMismatch(f"Physical indexes cover only {pos} of {len(self)} QTT cores")
+        merged = [_merge_cores(self.cores[p:p + n]) for p, n in groups]
+        return TensorTrain._wrap(merged).truncate(error=error, max_rank=max_rank)
+
     def __str__(self):
         return (f"{self.tt_type.value} with following properties:\n\t Number of cores: "
                 f"{len(self)}\n\t Bonds: {self.bonds}\n\t Physical indexes: "
@@ -409,6 +512,27 @@ def _apply_left(matrix: torch.Tensor, core: torch.Tensor) -> torch.Tensor:
                       device="cuda")
     K.gemm(matrix, core.reshape(core.shape[0], -1), out.view(matrix.shape[0], -1))
     return out
+
+
+def _merge_cores(cores: List[torch.Tensor]) -> torch.Tensor:
+    """Product of consecutive cores as one core (``tensor_train.py:57-92``):
+    each step multiplies the (left * rows * cols, bond) unfolding of the
+    running product by the next core's (bond, rest) unfolding, then moves
+    the new row factor in front of the running column factor."""
+    acc = cores[0]
+    for c in cores[1:]:
+        lb, R, C, b = acc.shape
+        _, r, s, rb = c.shape
+        prod = K.matmul(acc.reshape(-1, b), c.reshape(b, -1))
+        if C > 1 and r > 1:
+            out = K.empty(lb * R * r * C * s * rb)
+            tail = s * rb
+            K.copy_(out.view(lb * R, r, C, tail),
+                    prod.view(-1).as_strided((lb * R, r, C, tail),
+                                             (C * r * tail, tail, r * tail, 1)))
+            prod = out
+        acc = prod.view(lb, R * r, C * s, rb)
+    return acc
 
 
 def _apply_right(core: torch.Tensor, matrix: torch.Tensor) -> torch.Tensor:
