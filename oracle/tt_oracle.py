@@ -884,6 +884,156 @@ def als(A: Train, b: Train, x0: Optional[Train] = None, max_sweeps=4, residual_t
     return x, info
 
 
+def local_rhs_pair(left_b, b1, b2, right_b) -> np.ndarray:
+    """Two-site right-hand side (``solvers/two_site.py:28-49``), indexed
+    (frame bond, mode k, mode k+1, frame bond) and flattened."""
+    t = np.tensordot(left_b, b1[:, :, 0, :], axes=(0, 0))        # (i, j, b)
+    t = np.tensordot(t, b2[:, :, 0, :], axes=(2, 0))             # (i, j, k, c)
+    return np.tensordot(t, right_b, axes=(3, 0)).reshape(-1)     # (i, j, k, l)
+
+
+def local_matrix_pair(left_A, A1, A2, right_A) -> np.ndarray:
+    """Explicit two-site operator (``solvers/two_site.py:52-79``): rows
+    (frame bond, row k, row k+1, frame bond), columns the target side."""
+    t = np.einsum("iaj,aklb,bmnc,ocp->jkmpilno", left_A, A1, A2, right_A, optimize="optimal")
+    rows = left_A.shape[2] * A1.shape[1] * A2.shape[1] * right_A.shape[2]
+    return t.reshape(rows, -1)
+
+
+def local_operator_pair(left_A, A1, A2, right_A):
+    """Matrix-free two-site operator (``solvers/two_site.py:82-127``): the
+    right environment, the two operator cores and the left environment are
+    contracted into the block one after the other."""
+    shape = (left_A.shape[0], A1.shape[2], A2.shape[2], right_A.shape[0])
+    size = int(np.prod(shape))
+
+    def matmat(block):
+        y = np.asarray(block).reshape(shape + (-1,))
+        t = np.tensordot(y, right_A, axes=(3, 0))                 # (i, l, n, z, c, p)
+        t = np.tensordot(t, A2, axes=((2, 4), (2, 3)))           # (i, l, z, p, b, m)
+        t = np.tensordot(t, A1, axes=((1, 4), (2, 3)))           # (i, z, p, m, a, k)
+        t = np.tensordot(t, left_A, axes=((0, 4), (0, 1)))       # (z, p, m, k, j)
+        return t.transpose(4, 3, 2, 1, 0).reshape(size, -1)
+
+    return spla.LinearOperator(
+        (size, size), matvec=lambda v: matmat(v).ravel(), matmat=matmat, dtype=np.float64
+    )
+
+
+def _pair_warm_start(x: Train, k: int, center):
+    """Current supercore of sites k, k+1 (``solvers/two_site.py:130-153``),
+    with the block left by the last split in place of its stale core."""
+    left, right = x.cores[k][:, :, 0, :], x.cores[k + 1][:, :, 0, :]
+    if center is not None:
+        if center[0] == k:
+            left = center[1]
+        elif center[0] == k + 1:
+            right = center[1]
+    if left.shape[-1] != right.shape[0]:
+        return None
+    return np.tensordot(left, right, axes=(2, 0)).reshape(-1)
+
+
+def _local_solve_two_site(k, x, A, b, bonds, E, st: Settings, error_threshold, max_rank, damp,
+                          center, info: Info):
+    """``_solve_local_two_site`` (``solvers/two_site.py:156-241``): solve the
+    projected system of the supercore, split it by SVD and pick the rank of
+    the shared bond.  Returns (U, S, Vh, rank)."""
+    rows, cols = bonds[k] * x.row_modes[k], x.row_modes[k + 1] * bonds[k + 2]
+    size = rows * cols
+    b_loc = local_rhs_pair(E["lb"][k], b.cores[k], b.cores[k + 1], E["rb"][k + 1])
+    ops = (E["lA"][k], A.cores[k], A.cores[k + 1], E["rA"][k + 1])
+    iterative = st.iterative is not None and size > st.direct_solve_size
+    if iterative:
+        operator = local_operator_pair(*ops)
+        warm = _pair_warm_start(x, k, center)
+        if warm is not None and warm.size != size:
+            warm = None
+        fallback = (lambda: local_matrix_pair(*ops)) if st.allow_dense_fallback else None
+    else:
+        operator, warm, fallback = local_matrix_pair(*ops), None, None
+    u, operator = solve_local(operator, b_loc, st, iterative, warm, fallback, info)
+    exact = float(np.linalg.norm(operator @ u - b_loc)) if st.residual_mode else 0.0
+    U, S, Vh = sla.svd(u.reshape(rows, cols), full_matrices=False, check_finite=False,
+                       lapack_driver="gesvd")
+    if st.residual_mode:
+        rank = rank_by_residual(operator, b_loc, U, S, Vh, exact, st.truncation_tol, damp, max_rank)
+    else:
+        rank = rank_by_threshold(S, error_threshold, max_rank)
+    return U, S, Vh, rank
+
+
+def mals(A: Train, b: Train, x0: Optional[Train] = None, max_rank=None, max_sweeps=2,
+         residual_tol=None, residual_damp=2.0, stagnation_factor="auto", error_threshold=1e-7,
+         local_solver="auto", direct_solve_size=1000, local_rtol=None, allow_dense_fallback=False,
+         symmetric=False, return_info=True):
+    """MALS two-site sweeps (``solvers/mals.py:61-292``).  Left to right
+    the supercores of sites (k, k+1), k < d - 2, are solved and split, the
+    left factor kept as core k and the right factor held as the warm-start
+    block of site k+1; right to left every pair is solved again, the right
+    factor kept as core k+1 (and the left factor times S as core 0 at the
+    end).  The truncation budget is shared by 2d - 3 splits per sweep.
+    Returns ``(x, info)``."""
+    if max_rank is not None and max_rank <= 0:
+        raise ValueError(f"max_rank must be a positive integer, got {max_rank}")
+    if residual_damp < 1.0:
+        raise ValueError(f"residual_damp must be >= 1, got {residual_damp}")
+    d = len(A)
+    st = resolve_settings(max_sweeps, residual_tol, stagnation_factor, local_solver, symmetric,
+                          direct_solve_size, return_info, local_rtol, allow_dense_fallback,
+                          max(2 * d - 3, 1))
+    if x0 is None:
+        x0 = ones(b.row_modes, ranks=b.bonds)
+    x = x0.copy()
+    if x.orth_center != 0:
+        orthonormalize(x, "right")
+    E = {name: [None] * d for name in ("lA", "rA", "lb", "rb")}
+    for i in range(d - 1, 0, -1):  # mals.py:196-198
+        env_right(E["rA"], i, x, x, A)
+        env_right(E["rb"], i, x, b)
+    bonds = list(x.bonds)
+    info = Info()
+    b_norm = tt_norm(b) if st.track_residual else None
+    center = None
+    args = (st, error_threshold, max_rank, residual_damp)
+    for sweep in range(st.max_sweeps):
+        for k in range(d - 1):  # mals.py:216-249
+            env_left(E["lA"], k, x, x, A)
+            env_left(E["lb"], k, x, b)
+            if k == d - 2:
+                continue
+            U, S, Vh, nb = _local_solve_two_site(k, x, A, b, bonds, E, *args, center, info)
+            center = (k + 1, (S[:nb, None] * Vh[:nb]).reshape(nb, x.row_modes[k + 1],
+                                                                bonds[k + 2]))
+            x.cores[k] = U[:, :nb].reshape(bonds[k], x.row_modes[k], 1, nb)
+            bonds[k + 1] = nb
+            x.orth_center = k + 1
+        for k in range(d - 2, -1, -1):  # mals.py:252-283
+            env_right(E["rA"], k + 1, x, x, A)
+            env_right(E["rb"], k + 1, x, b)
+            U, S, Vh, nb = _local_solve_two_site(k, x, A, b, bonds, E, *args, center, info)
+            us = U[:, :nb] * S[:nb]
+            center = (k, us.reshape(bonds[k], x.row_modes[k], nb))
+            x.cores[k + 1] = Vh[:nb].reshape(nb, x.row_modes[k + 1], 1, bonds[k + 2])
+            bonds[k + 1] = nb
+            if k == 0:
+                x.cores[0] = us.reshape(bonds[0], x.row_modes[0], 1, nb)
+            x.orth_center = k
+        info.num_sweeps_run = sweep + 1
+        info.max_bonds.append(max(bonds))
+        if st.track_residual:
+            res = relative_residual(A, b, x, b_norm=b_norm)
+            info.residuals.append(res)
+            if st.residual_tol is not None and res <= st.residual_tol:
+                info.stop_reason = "converged"
+                break
+            if (st.stagnation_factor is not None and len(info.residuals) >= 2
+                    and info.residuals[-1] > st.stagnation_factor * info.residuals[-2]):
+                info.stop_reason = "stagnated"
+                break
+    return x, info
+
+
 def tt_svd(tensor: np.ndarray, error: float = 1e-12, max_rank=None, physical_indexes=None,
            ttm: bool = False) -> Train:
     """TT-SVD (``tensor_train.py:1138-1247``): left to right, the unfolding

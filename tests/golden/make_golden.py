@@ -5,6 +5,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
 
     python tests/golden/make_golden.py          # every case
     python tests/golden/make_golden.py als      # the ALS cases only
+    python tests/golden/make_golden.py mals     # the MALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
     python tests/golden/make_golden.py tt_svd   # TT-SVD only
     python tests/golden/make_golden.py tt_to_qtt  # quantisation only
@@ -125,6 +126,35 @@ def als_cases() -> None:
     amen_case("als_nonsym_gmres", A, b, solver=als, max_sweeps=4, direct_solve_size=4)
 
 
+def mals_cases() -> None:
+    """MALS (ttnumpy/solvers/mals.py with two_site.py): two-site sweeps
+    with rank adaptation at every split."""
+    from ttnumpy.solvers.mals import mals
+
+    # QTT Laplacian, residual-budget truncation, direct local solves
+    A, _ = qtt_laplacian_1d(6)
+    b = tt.ones([2] * 6)
+    amen_case("mals_qtt_lap1d_o6", A, b, solver=mals, residual_tol=1e-8, max_sweeps=6,
+              symmetric=True)
+    # 4-D Laplacian, threshold truncation with a rank cap, MINRES local solves
+    A = ref_train(P.laplacian_nd(4, 8))
+    b = tt.rand([8] * 4, ranks=2, seed=0)
+    amen_case("mals_lap4_minres", A, b, solver=mals, error_threshold=1e-6, max_rank=6,
+              max_sweeps=3, symmetric=True, direct_solve_size=100)
+    # QTT Laplacian of order 8 with a random right-hand side, rank cap 3
+    A, _ = qtt_laplacian_1d(8)
+    b = tt.rand([2] * 8, ranks=3, seed=4)
+    amen_case("mals_qtt_cap3", A, b, solver=mals, residual_tol=1e-10, max_rank=3, max_sweeps=4,
+              symmetric=True)
+    # non-symmetric, GMRES local solves from the warm-start supercores
+    rng = np.random.default_rng(5)
+    mat = np.eye(32) + 0.3 * rng.random((32, 32))
+    A = tt.tt_svd(mat.reshape([2] * 10), physical_indexes=[(2, 2)] * 5, ttm=True, error=0)
+    b = tt.tt_svd(rng.random(32).reshape([2] * 5), error=0)
+    amen_case("mals_nonsym_gmres", A, b, solver=mals, residual_tol=1e-9, max_sweeps=4,
+              direct_solve_size=4)
+
+
 def randomized_cases() -> None:
     """truncate(method="randomized") (tensor_train.py:913-937 with
     utils.py:139-236): the sketch-then-orthogonalise rounding."""
@@ -235,6 +265,9 @@ def main() -> None:
         return
     if "als" in sys.argv[1:]:
         als_cases()
+        return
+    if "mals" in sys.argv[1:]:
+        mals_cases()
         return
     if "randomized" in sys.argv[1:]:
         randomized_cases()
@@ -353,6 +386,7 @@ def main() -> None:
     save("dot_residual", data, {})
 
     als_cases()
+    mals_cases()
     randomized_cases()
     tt_svd_cases()
     tt_to_qtt_cases()

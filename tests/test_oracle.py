@@ -76,6 +76,29 @@ def test_oracle_als_matches_reference(case):
     assert diff <= 1e-9
 
 
+MALS_CASES = ["mals_qtt_lap1d_o6", "mals_lap4_minres", "mals_qtt_cap3", "mals_nonsym_gmres"]
+
+
+@pytest.mark.parametrize("case", MALS_CASES)
+def test_oracle_mals_matches_reference(case):
+    """MALS (``solvers/mals.py``, ``two_site.py``): two-site solves and
+    splits, the same sweeps, stop reason, bonds and residual trace as the
+    reference."""
+    data = load_golden(case)
+    A, b = _train(data, "A"), _train(data, "b")
+    x0 = _train(data, "x0") if "x0_n" in data else None
+    x, info = O.mals(A, b, x0=x0, **data["args"])
+    ref_x = _train(data, "x")
+    assert info.num_sweeps_run == int(data["num_sweeps_run"])
+    assert info.stop_reason == str(data["stop_reason"])
+    assert x.bonds == list(data["bonds"])
+    assert info.max_bonds == list(data["max_bonds"])
+    assert info.local_solves == int(data["local_solves"])
+    np.testing.assert_allclose(info.residuals, data["residuals"], rtol=1e-6, atol=1e-14)
+    diff = O.tt_norm(O.add(x, O.scale(ref_x, -1.0))) / O.tt_norm(ref_x)
+    assert diff <= 1e-9
+
+
 @pytest.mark.parametrize("case", ["truncate_pair_u", "truncate_pair_g", "truncate_pair_maxrank",
                                   "truncate_pair_d16"])
 def test_oracle_truncate_matches_reference(case):

@@ -1,7 +1,7 @@
 """B200-native tensor-train solve path: AMEn, TT rounding, TTM-by-TT.
 
 Drop-in replacements for the reference entry points ``amen``, ``als``,
-``TensorTrain.truncate`` and ``TensorTrain.dot`` (ttnumpy 0.3.0), computed
+``mals``, ``TensorTrain.truncate`` and ``TensorTrain.dot`` (ttnumpy 0.3.0), computed
 by hand-written sm_100a kernels in ``libttb200.so`` (C ABI in
 ``include/ttb200.h``).  There is no CPU path: the entry points raise when
 the library or a CUDA device is missing.
@@ -18,6 +18,7 @@ from .solvers.common import (  # noqa: F401
 )
 from .solvers.als import als  # noqa: F401
 from .solvers.amen import amen  # noqa: F401
+from .solvers.mals import mals  # noqa: F401
 from .tensor_train import (  # noqa: F401
     AmbiguousFormat,
     DimensionMismatch,
@@ -33,7 +34,7 @@ from .tensor_train import (  # noqa: F401
 )
 
 __all__ = [
-    "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen", "als",
+    "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen", "als", "mals",
     "SolverInfo", "StopReason", "LocalSolver", "TruncationMode", "relative_residual",
     "DimensionMismatch", "WrongTTFormat", "WrongTTType", "AmbiguousFormat", "tt_svd",
 ]

@@ -151,41 +151,61 @@ class _Sweeper:
 
     # -- local algebra ------------------------------------------------------
 
+    # The local system at site k is described by four hooks, so that a
+    # two-site sweep can reuse every local step with a merged supercore.
+
+    def op(self, k: int):
+        """(left environment, operator core, right environment) of the local
+        operator at site k."""
+        return self.left["A"][k], self.A.cores[k], self.right["A"][k]
+
+    def rhs_parts(self, k: int):
+        """(left environment, right-hand-side core, right environment) of
+        the local right-hand side at site k."""
+        return self.left["b"][k], _c3(self.b.cores[k]), self.right["b"][k]
+
+    def local_shape(self, k: int) -> Tuple[int, int, int]:
+        c = self.x.cores[k]
+        return c.shape[0], c.shape[1], c.shape[3]
+
+    def warm_start(self, k: int, u: torch.Tensor) -> bool:
+        """Fill ``u`` with the Krylov initial guess; False starts from zero."""
+        K.copy_(u, _c3(self.x.cores[k]))  # the current centre core
+        return True
+
     def local_rhs(self, k: int) -> torch.Tensor:
-        rl, rr = self.x.cores[k].shape[0], self.x.cores[k].shape[3]
-        n = self.x.cores[k].shape[1]
-        out = K.empty(rl, n, rr)
-        K.project([K.project_desc(self.left["b"][k], _c3(self.b.cores[k]), self.right["b"][k],
-                                  out)])
+        out = K.empty(*self.local_shape(k))
+        left, core, right = self.rhs_parts(k)
+        K.project([K.project_desc(left, core, right, out)])
         return out
 
     def apply_A(self, k: int, u: torch.Tensor, out: torch.Tensor, cols: int = 1, alpha=1.0,
                 beta=0.0) -> torch.Tensor:
-        K.local_apply([K.local_desc(self.left["A"][k], self.A.cores[k], self.right["A"][k], u, out,
-                                    cols, alpha, beta)])
+        left, core, right = self.op(k)
+        K.local_apply([K.local_desc(left, core, right, u, out, cols, alpha, beta)])
         return out
 
     def solve_local(self, k: int, stats: _Stats) -> Tuple[torch.Tensor, torch.Tensor]:
         """``_solve_local_one_site`` + ``_solve_local_system``
         (``one_site.py:118-178``, ``common.py:729-809``)."""
-        x = self.x
-        rl, n, rr = x.cores[k].shape[0], x.cores[k].shape[1], x.cores[k].shape[3]
-        size = rl * n * rr
+        shape = self.local_shape(k)
+        size = shape[0] * shape[1] * shape[2]
         b_loc = self.local_rhs(k)
         st = self.st
         if not st.use_iterative(size):
             return self._direct(k, b_loc), b_loc
         method = "minres" if st.iterative_solver is LocalSolver.MINRES else "gmres"
-        u = K.empty(rl, n, rr)
-        K.copy_(u, _c3(x.cores[k]))  # warm start: the current centre core
-        warm = True
+        u = K.empty(*shape)
+        warm = self.warm_start(k, u)
+        if not warm:
+            K.fill_(u, 0.0)
         rtol = st.local_rtol
         nb = K.empty(2)
         K.norm_into(nb[0:1], b_loc)
-        tmp = K.empty(rl, n, rr)
+        tmp = K.empty(*shape)
+        left, core, right = self.op(k)
         for _ in range(_MAX_LOCAL_RESTARTS):
-            K.krylov(method, self.left["A"][k], self.A.cores[k], self.right["A"][k], b_loc, u,
-                     rtol, warm)
+            K.krylov(method, left, core, right, b_loc, u, rtol, warm)
             warm = True
             self.apply_A(k, u, tmp)
             K.norm_into(nb[1:2], tmp, b_loc)
@@ -202,7 +222,7 @@ class _Sweeper:
         return self._direct(k, b_loc), b_loc
 
     def _direct(self, k: int, b_loc: torch.Tensor) -> torch.Tensor:
-        M = K.local_matrix(self.left["A"][k], self.A.cores[k], self.right["A"][k])
+        M = K.local_matrix(*self.op(k))
         u = _take(b_loc)
         info = torch.zeros(1, dtype=torch.int32, device="cuda")
         K.lu_solve_(M, u.reshape(-1), info)
