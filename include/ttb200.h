@@ -282,6 +282,21 @@ typedef struct {
 int ttb_kron(const ttb_kron_t* problems, int count, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Element-wise (Hadamard) product core, replacing the einsum of
+ * TensorTrain.multiply for two trains (ttnumpy/tensor_train.py:380-395):
+ *   out[(a, x), p, (b, y)] = lhs[a, p, b] * rhs[x, p, y]
+ * lhs (ra, modes, ra2), rhs (rx, modes, rx2), out (ra*rx, modes, ra2*rx2),
+ * with modes = row mode * column mode of the core.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  const double* lhs;
+  const double* rhs;
+  double* out;
+  int ra, ra2, rx, rx2, modes;
+} ttb_hadamard_t;
+int ttb_hadamard(const ttb_hadamard_t* problems, int count, void* stream);
+
+/* ------------------------------------------------------------------------
  * Sums of squares and norms.  out[p] = sqrt(sum of squares of x[0..n-1])
  * (the np.linalg.norm calls of the reference, e.g.
  * ttnumpy/tensor_train.py:529-538, ttnumpy/solvers/common.py:776,787),

@@ -349,6 +349,77 @@ def randomized_right_orth(cores: List[np.ndarray], rank: int, rng) -> List[np.nd
     return cores
 
 
+def hadamard(a: Train, b: Train) -> Train:
+    """Element-wise product of two trains (``tensor_train.py:380-395``):
+    core k is the Kronecker product of the two cores over the bonds,
+    indexed ((a, x), i, j, (b, y))."""
+    cores = []
+    for p, q in zip(a.cores, b.cores):
+        c = np.einsum("aijb,xijy->axijby", p, q)
+        cores.append(c.reshape(p.shape[0] * q.shape[0], p.shape[1], p.shape[2],
+                               p.shape[3] * q.shape[3]))
+    return Train(cores)
+
+
+def randomized_hadamard(lhs: List[np.ndarray], rhs: List[np.ndarray], rank: int, rng) -> List[np.ndarray]:
+    """HaTT-1 (``utils.py:262-333``): the randomised left orthonormalisation
+    of the element-wise product train without forming its cores.  The
+    sketch of the product right of each bond is built from one core of each
+    factor at a time (``utils.py:225-240``), the Gaussian cores drawn in the
+    order and shapes of the generic sketch, each sketch scaled by its
+    largest entry; left to right, the carried projection times the two
+    cores (``utils.py:243-259``) times the next sketch is factorised by QR."""
+    if rank < 1:
+        raise ValueError(f"rank must be positive, but got {rank}")
+    count = len(lhs)
+    sketches = [None] * count + [np.ones((1, 1, 1))]
+    for i in range(count - 1, 0, -1):
+        a, b = lhs[i], rhs[i]
+        m = a.shape[1] * a.shape[2]
+        contracted = np.einsum("apb,cpd,bdt->acpt", a.reshape(a.shape[0], m, a.shape[3]),
+                               b.reshape(b.shape[0], m, b.shape[3]), sketches[i + 1],
+                               optimize="optimal")
+        contracted = contracted.reshape(a.shape[0] * b.shape[0], -1)
+        bond = min(rank, *contracted.shape)
+        sketch = contracted @ rng.standard_normal((contracted.shape[1], bond))
+        top = np.abs(sketch).max()
+        if top > 0:
+            sketch /= top
+        sketches[i] = sketch.reshape(a.shape[0], b.shape[0], bond)
+    cores = []
+    carry = np.ones((1, 1, 1))
+    for i in range(count):
+        a, b = lhs[i], rhs[i]
+        m = a.shape[1] * a.shape[2]
+        matrix = np.einsum("tac,apb,cpd->tpbd", carry, a.reshape(a.shape[0], m, a.shape[3]),
+                           b.reshape(b.shape[0], m, b.shape[3]), optimize="optimal")
+        matrix = matrix.reshape(carry.shape[0] * m, -1)
+        shape = (carry.shape[0], a.shape[1], a.shape[2], -1)
+        if i == count - 1:
+            cores.append(matrix.reshape(shape))
+            break
+        q, _ = sla.qr(matrix @ sketches[i + 1].reshape(matrix.shape[1], -1), mode="economic")
+        cores.append(q.reshape(shape))
+        carry = (q.T @ matrix).reshape(q.shape[1], a.shape[3], b.shape[3])
+    return cores
+
+
+def multiply(a: Train, b: Train, truncate_: bool = False, error=None, max_rank=None,
+             method: str = "direct", seed=None, options=None) -> Train:
+    """``TensorTrain.multiply`` of two trains (``tensor_train.py:327-407``):
+    the product train, rounded when ``truncate_``; the randomized rounding
+    goes through HaTT-1 and the SVD sweep."""
+    if truncate_ and method == "randomized":
+        out = Train(randomized_hadamard(a.cores, b.cores, sketch_rank(max_rank, options),
+                                        np.random.default_rng(seed)), orth_center=len(a) - 1)
+        return compress_svd(out, 0.0 if error is None else error, max_rank)
+    out = hadamard(a, b)
+    if not truncate_:
+        return out
+    return truncate(out, 0.0 if error is None else error, max_rank, method=method, seed=seed,
+                    options=options)
+
+
 def truncate(t: Train, error: float = 0.0, max_rank=None, canonical="auto", method="direct",
              seed=None, options=None) -> Train:
     """TT rounding (``tensor_train.py:852-940``): QR (``method='direct'``)

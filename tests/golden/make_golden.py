@@ -7,6 +7,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
     python tests/golden/make_golden.py als      # the ALS cases only
     python tests/golden/make_golden.py mals     # the MALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
+    python tests/golden/make_golden.py hadamard # element-wise products only
     python tests/golden/make_golden.py tt_svd   # TT-SVD only
     python tests/golden/make_golden.py tt_to_qtt  # quantisation only
 
@@ -187,6 +188,38 @@ def randomized_cases() -> None:
     save("truncate_randomized", data, {"cases": [[n, kw] for n, kw in cases]})
 
 
+def hadamard_cases() -> None:
+    """TensorTrain.multiply of two trains (tensor_train.py:327-407): the
+    element-wise product, its direct rounding and HaTT-1 (utils.py:262-333)
+    for the randomized one."""
+    data = {}
+    g = np.random.default_rng(51)
+    cases = []
+    rp, rq = [1] + [3] * 5 + [1], [1] + [4] * 5 + [1]
+    p = tt.TensorTrain([g.standard_normal((rp[k], 3, 1, rp[k + 1])) for k in range(6)])
+    q = tt.TensorTrain([g.standard_normal((rq[k], 3, 1, rq[k + 1])) for k in range(6)])
+    pack(data, "p", p)
+    pack(data, "q", q)
+    for name, kw in [("plain", {}),
+                     ("direct", dict(truncate=True, error=1e-10)),
+                     ("rand_exact", dict(truncate=True, method="randomized", max_rank=12, seed=3)),
+                     ("rand_lossy", dict(truncate=True, method="randomized", max_rank=5, seed=4,
+                                         options={"oversampling": 0})),
+                     ("rand_err", dict(truncate=True, method="randomized", error=1e-2, max_rank=8,
+                                       seed=5))]:
+        pack(data, f"out_{name}", p.multiply(q, **kw))
+        cases.append([name, "p", "q", kw])
+    ra, rb = [1] + [2] * 4 + [1], [1] + [3] * 4 + [1]
+    A = tt.TensorTrain([g.standard_normal((ra[k], 2, 3, ra[k + 1])) for k in range(5)])
+    B = tt.TensorTrain([g.standard_normal((rb[k], 2, 3, rb[k + 1])) for k in range(5)])
+    pack(data, "A", A)
+    pack(data, "B", B)
+    kw = dict(truncate=True, method="randomized", max_rank=6, seed=6)
+    pack(data, "out_ttm", A.multiply(B, **kw))
+    cases.append(["ttm", "A", "B", kw])
+    save("hadamard", data, {"cases": cases})
+
+
 def tt_svd_cases() -> None:
     """tt_svd (tensor_train.py:1138-1247): the dense-to-TT builder."""
     data = {}
@@ -259,6 +292,9 @@ def tt_to_qtt_cases() -> None:
 def main() -> None:
     if "tt_to_qtt" in sys.argv[1:]:
         tt_to_qtt_cases()
+        return
+    if "hadamard" in sys.argv[1:]:
+        hadamard_cases()
         return
     if "tt_svd" in sys.argv[1:]:
         tt_svd_cases()
@@ -388,6 +424,7 @@ def main() -> None:
     als_cases()
     mals_cases()
     randomized_cases()
+    hadamard_cases()
     tt_svd_cases()
     tt_to_qtt_cases()
 

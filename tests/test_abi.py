@@ -39,6 +39,7 @@ def test_struct_sizes_match_c():
              "ttb_local_matrix_t": _lib.LocalMatrix, "ttb_project_t": _lib.Project,
              "ttb_qr_t": _lib.QR, "ttb_svd_t": _lib.SVD, "ttb_lu_t": _lib.LU,
              "ttb_copy_t": _lib.Copy, "ttb_kron_t": _lib.Kron, "ttb_norm_t": _lib.Norm,
+             "ttb_hadamard_t": _lib.Hadamard,
              "ttb_rank_t": _lib.Rank, "ttb_rank_rule_t": _lib.RankRule,
              "ttb_krylov_t": _lib.Krylov, "ttb_round_t": _lib.Round,
              "ttb_amen_task_t": _lib.AmenTask}

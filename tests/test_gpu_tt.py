@@ -295,3 +295,54 @@ def test_qtt_errors(tt):
     qm = tt.rand([(4, 4), (4, 4)], ranks=3, seed=126).tt_to_qtt(error=1e-12)
     with pytest.raises(tt.DimensionMismatch):
         qm.qtt_to_tt([(4, 2), (4, 8)])
+
+
+def test_multiply_matches_reference(tt):
+    """Element-wise product of two trains on the device against the
+    reference's results (``tensor_train.py:327-407``): the plain product
+    (``ttb_hadamard`` cores, exact), its direct rounding, and HaTT-1
+    randomized rounding (``utils.py:262-333``) with exact and lossy
+    sketches, an error bound and a TTM pair, drawn from the same seeds."""
+    data = load_golden("hadamard")
+    for name, a, b, kw in data["args"]["cases"]:
+        ac, _ = golden_train(data, a)
+        bc, _ = golden_train(data, b)
+        ref_c, ref_oc = golden_train(data, f"out_{name}")
+        out = tt.TensorTrain(ac).multiply(tt.TensorTrain(bc), **kw)
+        assert out.bonds == O.Train(ref_c).bonds, name
+        assert out.orth_center == ref_oc, name
+        if name == "plain":
+            assert all(np.array_equal(x, y) for x, y in zip(out.to_numpy(), ref_c)), name
+        got, want = O.Train(out.to_numpy()).full(), O.Train(ref_c).full()
+        assert np.linalg.norm(got - want) <= 1e-9 * np.linalg.norm(want), name
+
+
+def test_hattt_equals_sketch_of_formed_product(tt):
+    """HaTT-1 without the product cores gives the randomized left
+    orthonormalisation of the formed product train (same draws)."""
+    from ttnumpy_b200 import tensor_train as T
+
+    p = tt.rand([3] * 6, ranks=4, seed=1)
+    q = tt.rand([3] * 6, ranks=5, seed=2)
+    formed = [tt.kernels.hadamard(a, b) for a, b in zip(p.cores, q.cores)]
+    ref = T.randomized_left_orth(list(formed), 9, np.random.default_rng(7))
+    got = T.randomized_hadamard(p.cores, q.cores, 9, np.random.default_rng(7))
+    assert [c.shape for c in got] == [c.shape for c in ref]
+    a = O.Train([c.cpu().numpy() for c in got]).full()
+    b = O.Train([c.cpu().numpy() for c in ref]).full()
+    assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b)
+    for c in got[:-1]:
+        m = c.reshape(-1, c.shape[-1]).cpu().numpy()
+        assert np.allclose(m.T @ m, np.eye(m.shape[1]), atol=1e-12)
+
+
+def test_multiply_errors(tt):
+    p = tt.rand([3] * 4, ranks=2, seed=1)
+    with pytest.raises(tt.DimensionMismatch):
+        p.multiply(tt.rand([2] * 4, ranks=2, seed=1))
+    with pytest.raises(ValueError):
+        p.multiply(p, method="randomized")
+    with pytest.raises(ValueError):
+        p.multiply(p, truncate=True, method="randomized", max_rank=0)
+    with pytest.raises(TypeError):
+        p.multiply("x")

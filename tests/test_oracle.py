@@ -256,3 +256,19 @@ def test_oracle_qtt_round_trip_and_errors():
     for bad in ([4, 4], [8, 8, 8], [3, 8, 8]):
         with pytest.raises(ValueError):
             O.qtt_to_tt(q, bad)
+
+
+def test_oracle_multiply_matches_reference():
+    """Element-wise product of two trains (``tensor_train.py:327-407``):
+    plain, direct rounding, and HaTT-1 randomized rounding
+    (``utils.py:262-333``) with exact and lossy sketches and a TTM pair;
+    the same random draws, so the same cores up to rounding."""
+    data = load_golden("hadamard")
+    for name, a, b, kw in data["args"]["cases"]:
+        kw = dict(kw)
+        tr = kw.pop("truncate", False)
+        out = O.multiply(_train(data, a), _train(data, b), tr, **kw)
+        ref = _train(data, f"out_{name}")
+        assert out.bonds == ref.bonds, name
+        assert all(np.allclose(x, y, rtol=1e-8, atol=1e-10) for x, y in zip(out.cores, ref.cores)), name
+        assert out.orth_center == ref.orth_center, name

@@ -74,6 +74,11 @@ class Kron(C.Structure):
                 ("rx", I), ("rx2", I), ("kk", I)]
 
 
+class Hadamard(C.Structure):
+    _fields_ = [("lhs", P), ("rhs", P), ("out", P), ("ra", I), ("ra2", I), ("rx", I), ("rx2", I),
+                ("modes", I)]
+
+
 class Norm(C.Structure):
     _fields_ = [("x", P), ("y", P), ("out", P), ("n", L)]
 
@@ -136,6 +141,7 @@ _SIGNATURES = {
     "ttb_lu_solve": ([C.POINTER(LU), I, P], I),
     "ttb_copy": ([C.POINTER(Copy), I, P], I),
     "ttb_kron": ([C.POINTER(Kron), I, P], I),
+    "ttb_hadamard": ([C.POINTER(Hadamard), I, P], I),
     "ttb_norm": ([C.POINTER(Norm), I, P], I),
     "ttb_rank_work_doubles": ([L, I], L),
     "ttb_rank_residual": ([C.POINTER(Rank), I, P], I),

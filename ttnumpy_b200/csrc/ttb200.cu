@@ -244,6 +244,28 @@ __global__ void __launch_bounds__(TTB_THREADS) k_kron(const __grid_constant__ KB
   }
 }
 
+struct HBatch {
+  int count;
+  ttb_hadamard_t d[kMaxK];
+};
+
+// One output element per thread and step, written in order (coalesced
+// stores); the two factors' entries are re-read from L1/L2.
+__global__ void __launch_bounds__(TTB_THREADS) k_hadamard(const __grid_constant__ HBatch hb) {
+  const ttb_hadamard_t& q = hb.d[blockIdx.y];
+  const i64 total = (i64)q.ra * q.rx * q.modes * q.ra2 * q.rx2;
+  for (i64 e = (i64)blockIdx.x * TTB_THREADS + threadIdx.x; e < total;
+       e += (i64)gridDim.x * TTB_THREADS) {
+    i64 r = e;
+    int y = (int)(r % q.rx2); r /= q.rx2;
+    int b = (int)(r % q.ra2); r /= q.ra2;
+    int p = (int)(r % q.modes); r /= q.modes;
+    int x = (int)(r % q.rx); r /= q.rx;
+    int a = (int)r;
+    q.out[e] = q.lhs[((i64)a * q.modes + p) * q.ra2 + b] * q.rhs[((i64)x * q.modes + p) * q.rx2 + y];
+  }
+}
+
 constexpr int kMaxN = 64;
 struct NBatch {
   int count;
@@ -1640,6 +1662,26 @@ int ttb_kron(const ttb_kron_t* ps, int count, void* stream) {
     dim3 grid((unsigned)std::min<long long>(cdiv(most, TTB_THREADS), 2048), kb.count);
     ProfScope ps(P_KRON, s, 0.0, 0.0);
     k_kron<<<grid, TTB_THREADS, 0, s>>>(kb);
+    counted();
+  }
+  return last_error();
+}
+
+int ttb_hadamard(const ttb_hadamard_t* ps, int count, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  for (int i0 = 0; i0 < count; i0 += kMaxK) {
+    HBatch hb;
+    hb.count = std::min(kMaxK, count - i0);
+    long long most = 1;
+    for (int j = 0; j < hb.count; ++j) {
+      hb.d[j] = ps[i0 + j];
+      const ttb_hadamard_t& q = hb.d[j];
+      if (q.ra < 0 || q.ra2 < 0 || q.rx < 0 || q.rx2 < 0 || q.modes < 0) return (int)cudaErrorInvalidValue;
+      most = std::max(most, (long long)q.ra * q.rx * q.modes * q.ra2 * q.rx2);
+    }
+    dim3 grid((unsigned)std::min<long long>(cdiv(most, TTB_THREADS), 2048), hb.count);
+    ProfScope ps(P_KRON, s, 0.0, 0.0);
+    k_hadamard<<<grid, TTB_THREADS, 0, s>>>(hb);
     counted();
   }
   return last_error();

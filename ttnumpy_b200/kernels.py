@@ -305,6 +305,21 @@ def project(descs: List) -> None:
         check(lib().ttb_project(arr, len(descs), stream()), "ttb_project")
 
 
+def hadamard(lhs: torch.Tensor, rhs: torch.Tensor) -> torch.Tensor:
+    """Element-wise product core: out[(a,x), i, j, (b,y)] = lhs[a,i,j,b] rhs[x,i,j,y]."""
+    ra, n, m, ra2 = lhs.shape
+    rx, n_, m_, rx2 = rhs.shape
+    if (n_, m_) != (n, m):
+        raise ValueError("mode mismatch in element-wise product")
+    if not (lhs.is_contiguous() and rhs.is_contiguous()):
+        raise ValueError("element-wise product needs contiguous cores")
+    out = empty(ra * rx, n, m, ra2 * rx2)
+    d = _lib.Hadamard(ptr(lhs), ptr(rhs), ptr(out), ra, ra2, rx, rx2, n * m)
+    arr = (_lib.Hadamard * 1)(d)
+    check(lib().ttb_hadamard(arr, 1, stream()), "ttb_hadamard")
+    return out
+
+
 def kron(op: torch.Tensor, core: torch.Tensor) -> torch.Tensor:
     """TTM-by-TT core: out[(a,x), i, k, (b,y)] = sum_j op[a,i,j,b] core[x,j,k,y]."""
     ra, n, m, ra2 = op.shape

@@ -226,16 +226,30 @@ class TensorTrain:
 
     def multiply(self, other, truncate: bool = False, error=None, max_rank=None,
                  method: str = "direct", seed=None, options=None) -> "TensorTrain":
-        """Scalar multiple (``tensor_train.py:389-395``); the element-wise
-        product of two trains is not part of the solve path."""
+        """Element-wise product with a train or a scalar
+        (``tensor_train.py:327-407``).  Two trains: the product cores
+        (Kronecker over the bonds) come from ``ttb_hadamard``; with
+        ``truncate=True, method="randomized"`` they are never formed: HaTT-1
+        (:func:`randomized_hadamard`) gives the left-orthonormal cores of the
+        product, which the SVD sweep then truncates."""
+        if isinstance(other, TensorTrain):
+            if self.physical_dims() != other.physical_dims():
+                raise DimensionMismatch("Tensor trains must have the same dimensions")
+            if truncate and method == "randomized":
+                cores = randomized_hadamard(self.cores, other.cores,
+                                            _sketch_rank(max_rank, options),
+                                            np.random.default_rng(seed))
+                res = TensorTrain._wrap(cores, orth_center=len(cores) - 1)
+                return res.compress_svd(0.0 if error is None else error, max_rank, inplace=True)
+            cores = [K.hadamard(a.contiguous(), b.contiguous())
+                     for a, b in zip(self.cores, other.cores)]
+            return _round_result(TensorTrain._wrap(cores), truncate, error, max_rank, method,
+                                 seed, options)
         if isinstance(other, numbers.Number) and not isinstance(other, bool):
             res = self.copy()
             k = res.orth_center if res.orth_center is not None else 0
             K.copy_(res.cores[k], self.cores[k], float(other))
             return _round_result(res, truncate, error, max_rank, method, seed, options)
-        if isinstance(other, TensorTrain):
-            raise NotImplementedError("element-wise products of two trains are not on the "
-                                      "tensor-train solve path")
         raise TypeError(f"unsupported operand type(s) for *: 'TensorTrain' and '{type(other)}'")
 
     def __mul__(self, other):
@@ -604,6 +618,91 @@ def randomized_right_orth(cores: List[torch.Tensor], rank: int, rng) -> List[tor
     mirrored = [mirror(c) for c in reversed(cores)]
     randomized_left_orth(mirrored, rank, rng)
     cores[:] = [mirror(c) for c in reversed(mirrored)]
+    return cores
+
+
+def _hadamard_times_sketch(lhs: torch.Tensor, rhs: torch.Tensor,
+                           sketch: torch.Tensor) -> torch.Tensor:
+    """The product core of ``lhs`` (r, m, n, r') and ``rhs`` (s, m, n, s')
+    times ``sketch`` (r', s', l) over its right bond, as a (r * s, m n l)
+    matrix, without the product core (``utils.py:225-240``): one GEMM with
+    ``lhs``, one permuted copy, one GEMM per mode with ``rhs`` and a final
+    permuted copy into (r, s, modes, l) order."""
+    r, rr = lhs.shape[0], lhs.shape[3]
+    s, sr = rhs.shape[0], rhs.shape[3]
+    modes = lhs.shape[1] * lhs.shape[2]
+    ell = sketch.shape[2]
+    half = K.matmul(lhs.reshape(r * modes, rr), sketch.reshape(rr, sr * ell))
+    half = half.view(r, modes, sr, ell)
+    ht = K.empty(modes, sr, r, ell)  # (p, d, a, t)
+    K.copy_(ht, half.permute(1, 2, 0, 3))
+    full = K.empty(modes, s, r * ell)  # (p, c, (a, t))
+    K.gemm(rhs.reshape(s, modes, sr).permute(1, 0, 2), ht.view(modes, sr, r * ell), full)
+    out = K.empty(r, s, modes, ell)
+    K.copy_(out, full.view(modes, s, r, ell).permute(2, 1, 0, 3))
+    return out.view(r * s, modes * ell)
+
+
+def _carry_times_hadamard(carry: torch.Tensor, lhs: torch.Tensor,
+                          rhs: torch.Tensor) -> torch.Tensor:
+    """``carry`` (l, r, s) times the product core of ``lhs`` (r, m, n, r')
+    and ``rhs`` (s, m, n, s') over its left bond, as a (l m n, r' s')
+    matrix, without the product core (``utils.py:243-259``): one GEMM per
+    carry row with ``lhs``, one permuted copy, one GEMM per mode with
+    ``rhs`` and a final permuted copy into (l, modes, r', s') order."""
+    ell, r, s = carry.shape
+    rr, sr = lhs.shape[3], rhs.shape[3]
+    modes = lhs.shape[1] * lhs.shape[2]
+    half = K.empty(ell, s, modes * rr)  # (t, c, (p, b))
+    K.gemm(carry.permute(0, 2, 1), lhs.reshape(1, r, modes * rr), half)
+    ht = K.empty(modes, ell, rr, s)  # (p, t, b, c)
+    K.copy_(ht, half.view(ell, s, modes, rr).permute(2, 0, 3, 1))
+    full = K.empty(modes, ell * rr, sr)  # (p, (t, b), d)
+    K.gemm(ht.view(modes, ell * rr, s), rhs.reshape(s, modes, sr).permute(1, 0, 2), full)
+    out = K.empty(ell, modes, rr, sr)
+    K.copy_(out, full.view(modes, ell, rr, sr).permute(1, 0, 2, 3))
+    return out.view(ell * modes, rr * sr)
+
+
+def randomized_hadamard(lhs: List[torch.Tensor], rhs: List[torch.Tensor], rank: int,
+                        rng) -> List[torch.Tensor]:
+    """HaTT-1 (``randomized_hadamard``, ``utils.py:262-333``) on the device:
+    the randomized left orthonormalisation of the element-wise product of
+    two trains, never forming a product core.  Right to left, the product
+    right of each bond is contracted with a Gaussian train drawn on the host
+    from ``rng`` in the reference's order and shapes; left to right, the
+    carried projection times the two cores times the next sketch is
+    factorised by QR.  Sketches are scaled to unit norm (the reference
+    scales by the largest entry; the Q factors do not change)."""
+    if rank < 1:
+        raise ValueError(f"rank must be positive, but got {rank}")
+    count = len(lhs)
+    lhs = [c.contiguous() for c in lhs]
+    rhs = [c.contiguous() for c in rhs]
+    sketches: List[Optional[torch.Tensor]] = [None] * count + [K.fill_(K.empty(1, 1, 1), 1.0)]
+    nrm = K.empty(1)
+    for i in range(count - 1, 0, -1):
+        contracted = _hadamard_times_sketch(lhs[i], rhs[i], sketches[i + 1])
+        bond = min(rank, *contracted.shape)
+        gauss = torch.from_numpy(rng.standard_normal((contracted.shape[1], bond))).to("cuda")
+        sk = K.matmul(contracted, gauss)
+        K.norm_into(nrm, sk)
+        scale = float(nrm.item())
+        if scale > 0:
+            K.copy_(sk, sk, alpha=1.0 / scale)
+        sketches[i] = sk.view(lhs[i].shape[0], rhs[i].shape[0], bond)
+    cores: List[torch.Tensor] = []
+    carry = K.fill_(K.empty(1, 1, 1), 1.0)
+    for i in range(count):
+        matrix = _carry_times_hadamard(carry, lhs[i], rhs[i])
+        n, m = lhs[i].shape[1], lhs[i].shape[2]
+        if i == count - 1:
+            cores.append(matrix.view(carry.shape[0], n, m, -1))
+            break
+        q, _ = K.qr(K.matmul(matrix, sketches[i + 1].reshape(matrix.shape[1], -1)),
+                    want_r=False)
+        cores.append(q.reshape(carry.shape[0], n, m, q.shape[1]))
+        carry = K.matmul(q.t(), matrix).view(q.shape[1], lhs[i].shape[3], rhs[i].shape[3])
     return cores
 
 
