@@ -275,6 +275,85 @@ static __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
+// Split-K product for a small output and a long K range (the V^T V and
+// V^T C products of the blocked factorisations: M, N <= 48, one of them <= 16,
+// K in the thousands), where the tiled pipeline would spend one
+// synchronised k-step per 16 of K on a mostly empty 64 x 64 tile.  Each warp
+// takes a contiguous K slice and accumulates the whole MI*8 x NJ*8 product
+// in DMMA fragments from direct global loads (32-byte runs along K), with no
+// block barrier in the loop; the eight partial products are then added in
+// warp order through ``scratch`` (TTB_WARPS * M * N doubles of shared
+// memory), so the result does not depend on scheduling.
+template <int MI, int NJ>
+static __device__ __noinline__ void cta_gemm_skinny(CMat A, CMat B, OMat C, int M, int N, int K,
+                                                    double alpha, double beta, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int mi = (M + 7) >> 3, nj = (N + 7) >> 3;
+  double acc[MI][NJ][2];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int kper = (((K + TTB_WARPS - 1) / TTB_WARPS) + 3) & ~3;
+  const int kb = warp * kper, ke = min(K, kb + kper);
+  const double* ap[MI];
+  const double* bp[NJ];
+  bool aok[MI], bok[NJ];
+#pragma unroll
+  for (int i = 0; i < MI; ++i) {
+    aok[i] = 8 * i + g < M;
+    ap[i] = A.p + (aok[i] ? (i64)(8 * i + g) * A.rs : 0);
+  }
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    bok[j] = 8 * j + g < N;
+    bp[j] = B.p + (bok[j] ? (i64)(8 * j + g) * B.cs : 0);
+  }
+#pragma unroll 4
+  for (int k0 = kb; k0 < ke; k0 += 4) {
+    const int kk = k0 + t;
+    const bool okk = kk < ke;
+    double av[MI], bv[NJ];
+#pragma unroll
+    for (int i = 0; i < MI; ++i) av[i] = (okk && aok[i]) ? ap[i][(i64)kk * A.cs] : 0.0;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) bv[j] = (okk && bok[j]) ? bp[j][(i64)kk * B.rs] : 0.0;
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+        if (i < mi && j < nj) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+  }
+  const int mn = M * N;
+  double* mine = scratch + (i64)warp * mn;
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = 8 * i + g, col = 8 * j + 2 * t + h;
+        if (r < M && col < N) mine[r * N + col] = acc[i][j][h];
+      }
+  __syncthreads();
+  for (int e = threadIdx.x; e < mn; e += TTB_THREADS) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < TTB_WARPS; ++w) v += scratch[(i64)w * mn + e];
+    const int r = e / N, col = e % N;
+    double* cp = C.p + C.row(r) + C.col(col);
+    v *= alpha;
+    if (beta != 0.0) v = fma(beta, *cp, v);
+    *cp = v;
+  }
+  __syncthreads();  // callers may reuse the scratch and read C right away
+}
+
+// Output shapes and K lengths that take the split-K path.
+constexpr int kSkinnyK = 128;
+static_assert(TTB_WARPS * 16 * 48 <= GSTAGES * GSTAGE_D, "split-K scratch must fit the ring");
+
 static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
                                                   double alpha, double beta, double* ring) {
   if (M <= 0 || N <= 0) return;
@@ -282,6 +361,14 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
   // K == 0 (C = beta * C), go through the one-stage tile
   if (K <= 0 || __isShared(A.p) || __isShared(B.p)) {
     cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
+    return;
+  }
+  if (K >= kSkinnyK && M <= 16 && N <= 48) {
+    cta_gemm_skinny<2, 6>(A, B, C, M, N, K, alpha, beta, ring);
+    return;
+  }
+  if (K >= kSkinnyK && M <= 48 && N <= 16) {
+    cta_gemm_skinny<6, 2>(A, B, C, M, N, K, alpha, beta, ring);
     return;
   }
   const int tid = threadIdx.x;
