@@ -145,6 +145,28 @@ def test_rank1_factorisation_self_check(pers):
     assert checks[0] > 0.0  # the diffusion solve truncated with residual-budget ranks
 
 
+def test_chunked_rank_search_matches_term_by_term(pers):
+    """Outside debug mode the rank search forms the applied rank-one terms
+    eight at a time (three GEMMs per chunk, the rank-R contraction fused
+    into the running-sum loop); debug mode keeps the term-by-term search.
+    Both must take the same rank decisions: same bonds and sweeps, residuals
+    and solutions equal to rounding."""
+    kw = dict(residual_tol=1e-8, symmetric=True, max_sweeps=4, seed=0, stagnation_factor=None)
+    reqs = [(p.A, p.b, None, kw) for p in (_diffusion(3, 4, 16), _diffusion(4, 3, 32),
+                                           P.qtt_poisson_2d(5))]
+    runs = []
+    for debug in (True, False):
+        batch = pers.PersistentBatch(pers.prepare(reqs), 64, debug=debug)
+        out = batch.run()
+        assert all(r.status == 0 for r in out)
+        runs.append(out)
+    for a, b in zip(*runs):
+        assert a.x.bonds == b.x.bonds
+        assert a.info.num_sweeps_run == b.info.num_sweeps_run
+        np.testing.assert_allclose(a.info.residuals, b.info.residuals, rtol=1e-6, atol=1e-14)
+        assert rel_tt(otrain(a.x), otrain(b.x)) < 1e-9
+
+
 def test_two_level_qr_self_check(pers):
     """The residual-norm sweep factorises tall matrices (rows >= 4 x columns,
     more than 64 columns) with the two-level blocked R-only QR; in debug mode

@@ -682,8 +682,41 @@ __device__ __noinline__ void rank1_apply(Ctx& c, const LocalOp& L, bool forward,
   c.top = mark;
 }
 
-// U (M x p, col stride p... row major M x p), S (p), Vh (p x Kc row major):
-// the solved core u = U diag(S) Vh as a vector of length M * Kc.
+// Ranks whose applied rank-one terms are formed together in choose_rank.
+constexpr int kRankChunk = 8;
+
+// The operator applied to the rank-one terms c0 .. c0+nc-1 of the solved
+// core at once (rank1_apply for a chunk): the per-term products become three
+// GEMMs over the whole chunk, and the last, rank-R contraction is left to the
+// caller's accumulation loop.  Forward split: Yc[(r, j), (k, b)] =
+// sum_{a, l} (sum_i left[i, a, j] U[(i, l), c0 + r]) op[a, k, l, b], to be
+// combined with Wall[c0 + r, (b, q)] = s sum_p' Vh[., p'] right[p', b, q].
+// Backward split: Zc[(a, k), (r, q)] = sum_{l, b} op[a, k, l, b]
+// (sum_p' Vh[c0 + r, (l, p')] right[p', b, q]), to be combined with
+// YV[c0 + r, (a, j)] = sum_i U[i, .] left[i, a, j].
+__device__ __noinline__ void rank_chunk(Ctx& c, const LocalOp& L, bool forward, const double* Up,
+                                        const double* Vh, int p, int c0, int nc, double* Y,
+                                        double* out) {
+  const int lt = L.lt, lf = L.lf, R = L.R, R2 = L.R2, n = L.n, m = L.m, rt = L.rt, rf = L.rf;
+  if (forward) {
+    // Y (PP2[r][j][a][l]) = left^T Up[:, c0:c0+nc, :], written permuted
+    gemm(c, CMat{L.left, 1, (i64)R * lf}, CMat{Up + (i64)c0 * m, (i64)p * m, 1},
+         OMat(Y, lf, m, (i64)R * m, m, (i64)lf * R * m, 1), R * lf, nc * m, lt, 1.0, 0.0);
+    // out[(r, j), (k, b)] = PP2[(r, j), (a, l)] opP[(a, l), (k, b)]
+    gemm(c, CMat{Y, (i64)R * m, 1}, CMat{L.opP, (i64)n * R2, 1}, Mat{out, (i64)n * R2, 1},
+         nc * lf, n * R2, R * m, 1.0, 0.0);
+  } else {
+    // Y (Qt[(l, b)][(r, q)]) = Vh[c0:c0+nc, (l, p')] right[p', (b, q)], written permuted
+    gemm(c, CMat{Vh + (i64)c0 * m * rt, rt, 1}, CMat{L.right, (i64)R2 * rf, 1},
+         OMat(Y, m, rf, (i64)R2 * nc * rf, rf, (i64)nc * rf, 1), nc * m, R2 * rf, rt, 1.0, 0.0);
+    // out[(a, k), (r, q)] = op[(a, k), (l, b)] Qt[(l, b), (r, q)]
+    gemm(c, CMat{L.op, (i64)m * R2, 1}, CMat{Y, (i64)nc * rf, 1}, Mat{out, (i64)nc * rf, 1},
+         R * n, nc * rf, m * R2, 1.0, 0.0);
+  }
+}
+
+// U (M x p row major), S (p), Vh (p x Kc row major): the solved core
+// u = U diag(S) Vh as a vector of length M * Kc.
 __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const double* b_loc, const double* U,
                            const double* S, const double* Vh, int M, int Kc, int p) {
   const ttb_amen_task_t* T = c.T;
@@ -705,7 +738,6 @@ __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const do
   permute_op(c, L);
   double* tmp = take(c, N);
   double* part = take(c, N);
-  double* term = take(c, N);
   if (c.status) return 1;
   apply(c, L, u, tmp, 1, 1.0, 0.0);
   const double exact = vnorm_diff(tmp, b_loc, N, red);
@@ -715,11 +747,13 @@ __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const do
   __syncthreads();
   int rank = limit;
   const bool forward = (M == L.lt * L.m);
-  for (int r = 0; r < limit; ++r) {
-    rank1_apply(c, L, forward, U, S, Vh, p, r, tmp);
+  if (T->debug) {
+    // one term at a time, each also applied in full for the self-check
+    double* term = take(c, N);
     if (c.status) return 1;
-    if (T->debug) {
-      // the full application of B to the term, for the self-check
+    for (int r = 0; r < limit; ++r) {
+      rank1_apply(c, L, forward, U, S, Vh, p, r, tmp);
+      if (c.status) return 1;
       const double sr = S[r];
       for (i64 e = threadIdx.x; e < N; e += TTB_THREADS) {
         i64 i = e / Kc, j = e % Kc;
@@ -747,16 +781,92 @@ __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const do
       c.check = fmax(c.check, worst);
       __syncthreads();
       c.top -= ((N + 31) & ~31LL);
+      double s = 0.0;
+      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+        double v = part[i] + tmp[i];
+        part[i] = v;
+        s = fma(v, v, s);
+      }
+      if (sqrt(block_sum(s, red)) <= thr) {
+        rank = r + 1;
+        break;
+      }
     }
-    double s = 0.0;
-    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
-      double v = part[i] + tmp[i];
-      part[i] = v;
-      s = fma(v, v, s);
+    c.top = mark;
+    return rank;
+  }
+  // Chunks of kRankChunk terms: their applications by rank_chunk, then the
+  // running sum -b + C_0 + ... + C_r and its norm term by term, in order, so
+  // the first rank within the budget is the one a term-by-term search finds.
+  const int lt = L.lt, lf = L.lf, R = L.R, R2 = L.R2, n = L.n, m = L.m, rf = L.rf, rt = L.rt;
+  const int CH = kRankChunk;
+  double* Up = nullptr;    // forward: Up[i][r][l] = U[(i, l), r]
+  double* side = nullptr;  // forward: Wall (limit x R2*rf); backward: YV (limit x R*lf)
+  double* Y = take(c, forward ? (i64)CH * lf * R * m : (i64)CH * m * R2 * rf);
+  double* Cc = take(c, forward ? (i64)CH * lf * n * R2 : (i64)R * n * CH * rf);
+  if (forward) {
+    Up = take(c, (i64)lt * p * m);
+    side = take(c, (i64)limit * R2 * rf);
+    double* svh = take(c, (i64)limit * rt);
+    if (c.status) return 1;
+    for (i64 e = threadIdx.x; e < (i64)lt * p * m; e += TTB_THREADS) {
+      const int l = (int)(e % m);
+      const int r = (int)((e / m) % p);
+      const i64 i = e / ((i64)m * p);
+      Up[e] = U[(i * m + l) * p + r];
     }
-    if (sqrt(block_sum(s, red)) <= thr) {
-      rank = r + 1;
-      break;
+    for (i64 e = threadIdx.x; e < (i64)limit * rt; e += TTB_THREADS) svh[e] = S[e / rt] * Vh[e];
+    __syncthreads();
+    gemm(c, CMat{svh, rt, 1}, CMat{L.right, (i64)R2 * rf, 1}, Mat{side, (i64)R2 * rf, 1}, limit,
+         R2 * rf, rt, 1.0, 0.0);
+  } else {
+    side = take(c, (i64)limit * R * lf);
+    if (c.status) return 1;
+    gemm(c, CMat{U, 1, p}, CMat{L.left, (i64)R * lf, 1}, Mat{side, (i64)R * lf, 1}, limit,
+         R * lf, lt, 1.0, 0.0);
+  }
+  if (c.status) return 1;
+  for (int c0 = 0; c0 < limit; c0 += CH) {
+    const int nc = min(CH, limit - c0);
+    rank_chunk(c, L, forward, Up, Vh, p, c0, nc, Y, Cc);
+    if (c.status) return 1;
+    for (int rr = 0; rr < nc; ++rr) {
+      const int r = c0 + rr;
+      double s = 0.0;
+      if (forward) {
+        // part[(j, k), q] += sum_b Cc[(rr, j, k), b] Wall[r, (b, q)]
+        const double* Yr = Cc + (i64)rr * lf * n * R2;
+        const double* Wr = side + (i64)r * R2 * rf;
+        for (unsigned e = threadIdx.x; e < (unsigned)N; e += TTB_THREADS) {
+          const unsigned jk = e / (unsigned)rf, q = e % (unsigned)rf;
+          const double* y = Yr + (i64)jk * R2;
+          double v = part[e];
+          for (int b = 0; b < R2; ++b) v = fma(y[b], Wr[(i64)b * rf + q], v);
+          part[e] = v;
+          s = fma(v, v, s);
+        }
+      } else {
+        // part[j, (k, q)] += s_r sum_a YV[r, (a, j)] Cc[(a, k), (rr, q)]
+        const double sr = S[r];
+        const double* yv = side + (i64)r * R * lf;
+        const unsigned nq = (unsigned)(n * rf);
+        for (unsigned e = threadIdx.x; e < (unsigned)N; e += TTB_THREADS) {
+          const unsigned j = e / nq;
+          const unsigned kq = e % nq;
+          const unsigned kk = kq / (unsigned)rf, q = kq % (unsigned)rf;
+          double acc = 0.0;
+          for (int a = 0; a < R; ++a)
+            acc = fma(yv[(i64)a * lf + j], Cc[((i64)a * n + kk) * ((i64)nc * rf) + (i64)rr * rf + q],
+                      acc);
+          const double v = fma(sr, acc, part[e]);
+          part[e] = v;
+          s = fma(v, v, s);
+        }
+      }
+      if (sqrt(block_sum(s, red)) <= thr) {
+        c.top = mark;
+        return r + 1;
+      }
     }
   }
   c.top = mark;
@@ -1464,7 +1574,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   const long long dn = std::min<long long>(direct_solve_size, N);
   const long long direct = dn * dn + dn;
   const long long iter = N + 7 * N + apply;
-  const long long rank = 3 * N + apply;
+  const long long rank = 4 * N + 2LL * kRankChunk * R * n * r + R * r * r + r * r + apply;
   const long long fact = r * n * r + r + r * n * r        // U S Vh
                          + (r * n) * r + 2 * r * r + 4 * r  // svd work
                          + (r * n) * cols + 2 * cols * n * r + r * r  // enriched, padded, svh
