@@ -28,6 +28,12 @@ constexpr int kD = 64;                 // most cores per train
 constexpr int kPoolBytes = 160 * 1024;  // dynamic shared-memory pool (after the GEMM ring)
 constexpr int kRingBytes = GSTAGES * GSTAGE_D * 8;
 constexpr i64 kPoolD = kPoolBytes / 8;
+// fixed-size pool users: the two-level R-only QR's panel buffers and the
+// blocked factorisations' reflector chunk
+static_assert(kPoolD >= 3 * LNB2 * LNB2 + LNB * LNB2 + 2 * LNB * LNB, "pool too small");
+static_assert(kPoolD >= (i64)LNB * YCH + 2 * LNB * LNB, "pool too small");
+// ring + pool + the kernel's static shared memory (about 9 KB) within 227 KB
+static_assert(kRingBytes + kPoolBytes <= 216 * 1024, "dynamic shared memory over budget");
 constexpr int kMaxRestarts = 4;        // common.py:230
 constexpr double kShrink = 1e-2;       // common.py:233
 constexpr int kMaxMinres = 2000;       // iteration cap of one MINRES call

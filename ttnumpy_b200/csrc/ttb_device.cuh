@@ -363,13 +363,16 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
     cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
     return;
   }
-  if (K >= kSkinnyK && M <= 16 && N <= 48) {
-    cta_gemm_skinny<2, 6>(A, B, C, M, N, K, alpha, beta, ring);
-    return;
-  }
-  if (K >= kSkinnyK && M <= 48 && N <= 16) {
-    cta_gemm_skinny<6, 2>(A, B, C, M, N, K, alpha, beta, ring);
-    return;
+  // (operands contiguous along K only: the split-K loads read 32-byte runs of K)
+  if (K >= kSkinnyK && A.cs == 1 && B.rs == 1) {
+    if (M <= 16 && N <= 48) {
+      cta_gemm_skinny<2, 6>(A, B, C, M, N, K, alpha, beta, ring);
+      return;
+    }
+    if (M <= 48 && N <= 16) {
+      cta_gemm_skinny<6, 2>(A, B, C, M, N, K, alpha, beta, ring);
+      return;
+    }
   }
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
