@@ -54,6 +54,11 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="requests in the CPU baseline sample (0: automatic)")
+    ap.add_argument("--serve-requests", type=int, default=0,
+                    help="requests in the served stream (0: three times --requests, the "
+                         "batch's requests cycled)")
+    ap.add_argument("--serve-mem-gb", type=float, default=48.0,
+                    help="device memory the server may hold in slabs of requests in flight")
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="arrival rate of the served run (0: twice the measured batch rate)")
     ap.add_argument("--plain-sample", type=int, default=8,
@@ -494,32 +499,60 @@ def main():
 
 
 def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
-    """Timed region for the persistent engine: one launch per step."""
+    """Timed region for the persistent engine: one launch per step.  Steps
+    alternate between two device-resident copies of the batch on two
+    streams, so a step's last (longest-running) solves overlap the next
+    step's first ones, as back-to-back batches do in service; a copy is
+    launched again only after its previous step has been collected."""
     import torch
 
     from ttnumpy_b200 import kernels as K
 
-    step_ms, ok, launches, lats, flops = [], 0, 0, [], 0.0
+    batches = [batch, eng.upload(reqs)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    ok, lats, flops = 0, [], 0.0
+
+    def collect(j):
+        nonlocal ok, flops
+        with torch.cuda.stream(streams[j]):  # host reads on the batch's own stream
+            res = batches[j].collect()
+            lats.extend(batches[j].latencies_ms())
+            flops += batches[j].gemm_flops()
+        ok += sum(1 for r in res if r.status == 0 and r.info.converged)
+
     barrier()
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            K.fill_(flush, 0.0)
-            torch.cuda.synchronize()
-            l0 = K.launch_count()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            batch.launch()
-            e.record()
-            torch.cuda.synchronize()
-            launches += K.launch_count() - l0
-            ms = s.elapsed_time(e)
-            step_ms.append(ms)
-            res = batch.collect()
-            ok += sum(1 for r in res if r.status == 0 and r.info.converged)
-            lats.extend(batch.latencies_ms())
-            flops += batch.gemm_flops()
+        K.fill_(flush, 0.0)
+        torch.cuda.synchronize()
+        l0 = K.launch_count()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        done = [None, None]
+        for k in range(args.steps):
+            j = k % 2
+            if done[j] is not None:
+                done[j].synchronize()
+                collect(j)
+            streams[j].wait_event(start)
+            batches[j].launch(streams[j])
+            done[j] = torch.cuda.Event()
+            done[j].record(streams[j])
+        for k in range(max(0, args.steps - 2), args.steps):
+            done[k % 2].synchronize()
+            collect(k % 2)
+        cur = torch.cuda.current_stream()
+        for st in streams:
+            cur.wait_stream(st)
+        end = torch.cuda.Event(enable_timing=True)
+        end.record()
+        torch.cuda.synchronize()
+        launches = K.launch_count() - l0
+    step_ms = [start.elapsed_time(end)]
     barrier()
     value, total_ms = aggregate_rate(ok, sum(step_ms), world)
+    for b in batches:  # the served run admits its own requests by device memory
+        b.release()
+    torch.cuda.empty_cache()
     e2e = served_run(reqs, args, torch, rate=args.serve_rate or 2.0 * value / world)
     e2e["value"], _ = aggregate_rate(e2e.pop("_solved"), 1e3 * e2e.pop("_seconds"), world)
     plain = plain_run(reqs, args) if (world == 1 and args.plain_sample > 0) else None
@@ -536,7 +569,9 @@ def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
                               f"this workload (profiles/k_amen_bench_{args.requests}req.md)",
             "flops_counted": "2mnk of every dense product the blocks ran; QR/SVD/LU not counted",
-            "per_launch_us": 1e3 * sum(step_ms) / len(step_ms), "launches": len(step_ms)}
+            "per_launch_us": 1e3 * sum(step_ms) / args.steps, "launches": args.steps,
+            "timing": "aggregate over the timed steps (consecutive launches overlap on two "
+                      "streams)"}
     cpu = None
     if world == 1:
         n_sample = args.cpu_sample or min(len(reqs), max(2 * cpu_cores(), 8))
@@ -604,14 +639,17 @@ def served_run(reqs, args, torch, rate):
     each timed with CUDA events around the whole stream."""
     from ttnumpy_b200.persistent_serving import PersistentServer
 
-    host = [(p.A, p.b, Engine.x0_host(p), solve_kwargs(p)) for p in reqs]
+    n_serve = args.serve_requests or 3 * len(reqs)
+    batch_host = [(p.A, p.b, Engine.x0_host(p), solve_kwargs(p)) for p in reqs]
+    host = [batch_host[i % len(batch_host)] for i in range(n_serve)]
     rng = np.random.default_rng(args.seed + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(host)))
     arrivals -= arrivals[0]
-    seconds, solved, lats, launches, h2d, d2h = 0.0, 0, [], 0, 0, 0
+    budget = int(args.serve_mem_gb * 2**30)
+    seconds, solved, lats, launches, h2d, d2h, peak = 0.0, 0, [], 0, 0, 0, 0
     steps = max(1, args.steps)
     for _ in range(steps):
-        server = PersistentServer()
+        server = PersistentServer(mem_budget=budget)
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
@@ -624,11 +662,15 @@ def served_run(reqs, args, torch, rate):
         lats.extend(1e3 * j.latency for j in jobs)
         launches += server.launches
         h2d, d2h = server.h2d_bytes, server.d2h_bytes
+        peak = max(peak, server.peak_bytes)
     return {"value": solved / seconds, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h,
-            "mode": f"served: {len(reqs)} requests per step arriving as a Poisson stream at "
-                    f"{rate:.1f}/s, continuous batching over 16 streams of persistent launches, "
-                    "inputs copied from host per launch, solutions read back",
+            "mode": f"served: {len(host)} requests per step (the batch's {len(reqs)} cycled) "
+                    f"arriving as a Poisson stream at {rate:.1f}/s, continuous batching over 16 "
+                    f"streams of persistent launches admitted by a {args.serve_mem_gb:g} GB "
+                    "slab budget, inputs copied from host per launch, solutions read back",
+            "requests_per_step": len(host),
+            "peak_slab_gb": peak / 2**30,
             "launches_per_step": launches / steps,
             "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
             "_seconds": seconds, "_solved": solved}
@@ -696,7 +738,10 @@ def config(args, reqs, engine="reference"):
                         "residual 1e-8",
             "requests_per_step": len(reqs), "mix": kinds, "engine": engine,
             "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
-            "l2": "flushed (512 MB write) before every timed step",
+            "l2": "inputs larger than L2 (two batches of slabs, tens of GB); 512 MB flush "
+                  "before the timed region",
+            "steps": "alternate between two device-resident copies of the batch on two "
+                     "streams, so one step's last solves overlap the next step's first",
             "parallelism": f"replicas x{args.gpus}"}
 
 

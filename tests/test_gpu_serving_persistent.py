@@ -57,3 +57,27 @@ def test_staggered_arrivals_match_alone(srv_mod):
         (alone,) = pers.amen_persistent([(p.A, p.b, None, KW)])
         assert alone.info.residuals == res.info.residuals, p.name
         assert all(np.array_equal(u, v) for u, v in zip(alone.x.to_numpy(), job.host_cores))
+
+
+def test_memory_budget_admission(srv_mod):
+    """With a device-memory budget the server never holds more slab bytes
+    in flight than the budget (a request larger than the budget runs alone),
+    and the results are those of the unconstrained server."""
+    pers, ps = srv_mod
+    probs = _problems()
+    reqs = [(p.A, p.b, None, KW) for p in probs]
+    arrivals = [0.0] * len(reqs)  # one burst: everything queued at once
+    sizes = [8 * pers.slab_doubles(pers.prepare([r])[0], 64) for r in reqs]
+    budget = 2 * max(sizes)
+    server = ps.PersistentServer(streams=4, min_interval=0.0, mem_budget=budget)
+    jobs = server.serve(reqs, arrivals)
+    assert server.peak_bytes <= budget
+    assert server.launches >= 2  # the burst did not fit in one launch
+    free = ps.PersistentServer(streams=4, min_interval=0.0).serve(reqs, arrivals)
+    for p, a, b in zip(probs, jobs, free):
+        assert a.result.status == 0 and a.result.info.converged, p.name
+        assert a.result.info.residuals == b.result.info.residuals, p.name
+        assert all(np.array_equal(u, v) for u, v in zip(a.host_cores, b.host_cores))
+    tiny = ps.PersistentServer(streams=2, min_interval=0.0, mem_budget=1)
+    (job,) = tiny.serve(reqs[:1], [0.0])
+    assert job.result.status == 0 and tiny.launches == 1

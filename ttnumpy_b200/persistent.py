@@ -128,6 +128,18 @@ class _Prepared:
         return np.array(self.modes + R + rb + xb + zb, dtype=np.int32)
 
 
+def slab_doubles(p: "_Prepared", rmax: int) -> int:
+    """Device work area (doubles) of one request at slot capacity ``rmax``:
+    the kernel's own bound (``ttb_amen_slab_doubles``), rounded up to 64."""
+    dh = p.dims()
+    arr = (C.c_int * len(dh))(*dh.tolist())
+    size = _lib_handle().ttb_amen_slab_doubles(p.d, arr, p.kick, rmax,
+                                               int(min(p.st.direct_solve_size, 1 << 30)))
+    if size < 0:
+        raise ValueError("train too long for the persistent path")
+    return (size + 63) // 64 * 64
+
+
 class PersistentBatch:
     """Requests packed on the device for the persistent kernel.
 
@@ -156,14 +168,7 @@ class PersistentBatch:
         dims_host = [p.dims() for p in preps]
         dim_pos = np.cumsum([0] + [len(x) for x in dims_host])
         self.dev_dims = torch.from_numpy(np.concatenate(dims_host)).to("cuda")
-        sizes = []
-        for p, dh in zip(preps, dims_host):
-            arr = (C.c_int * len(dh))(*dh.tolist())
-            size = lib.ttb_amen_slab_doubles(p.d, arr, p.kick, rmax,
-                                             int(min(p.st.direct_solve_size, 1 << 30)))
-            if size < 0:
-                raise ValueError("train too long for the persistent path")
-            sizes.append((size + 63) // 64 * 64)
+        sizes = [slab_doubles(p, rmax) for p in preps]
         self.slab_pos = np.cumsum([0] + sizes)
         self.slabs = torch.empty(int(self.slab_pos[-1]), dtype=torch.float64, device="cuda")
         self.dmax = max(p.d for p in preps)
@@ -294,6 +299,19 @@ class PersistentBatch:
     def run(self, stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
         self.launch(stream)
         return self.collect()
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the batch holds: inputs, slabs and result tables."""
+        return sum(t.numel() * t.element_size() for t in
+                   (self.dev_in, self.dev_off, self.dev_dims, self.slabs, self.resid,
+                    self.result, self.xoff) if t is not None)
+
+    def release(self) -> None:
+        """Drop the device buffers (results already collected stay valid:
+        their cores were cloned out of the slabs)."""
+        self.dev_in = self.dev_off = self.dev_dims = self.slabs = None
+        self.resid = self.result = self.xoff = None
 
 
 def _cost(p: "_Prepared") -> float:

@@ -12,6 +12,12 @@ are read back when its completion event has fired.
 
 A request whose bonds outgrow the launch's slot capacity (status -4) is
 queued again with twice the capacity, as ``amen_persistent`` does.
+
+Requests are admitted by device memory: with ``mem_budget`` set, a launch
+takes waiting requests only while the work areas (slabs) of all launches in
+flight stay within the budget, so a burst of arrivals queues on the host
+instead of exhausting HBM.  A request larger than the whole budget is
+launched alone once nothing else is in flight.
 Latency is measured per request on the host clock, from arrival to the
 moment its launch is found complete.
 """
@@ -25,7 +31,7 @@ from typing import Callable, List, Optional, Sequence
 import torch
 
 from . import kernels as K
-from .persistent import PersistentBatch, Result, _cost, _Prepared
+from .persistent import PersistentBatch, Result, _cost, _Prepared, slab_doubles
 
 
 @dataclass
@@ -35,6 +41,7 @@ class Job:
     prep: _Prepared
     rmax: int
     result: Optional[Result] = None
+    slab_bytes: int = 0  # work area at the current slot capacity
     done_at: Optional[float] = None
     host_cores: Optional[list] = None  # the solution's cores read back to the host
 
@@ -53,7 +60,8 @@ class PersistentServer:
     """
 
     def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: int = 64,
-                 max_rmax: int = 256, min_interval: float = 0.005, download: bool = True):
+                 max_rmax: int = 256, min_interval: float = 0.005, download: bool = True,
+                 mem_budget: Optional[int] = None):
         K.device_ok()
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.free = list(range(streams))
@@ -62,8 +70,11 @@ class PersistentServer:
         self.max_rmax = max_rmax
         self.min_interval = min_interval
         self.download = download
+        self.mem_budget = mem_budget
+        self.inflight_bytes = 0
+        self.peak_bytes = 0
         self.queue: List[Job] = []
-        self.inflight = []  # (stream index, batch, event, jobs)
+        self.inflight = []  # (stream index, batch, event, jobs, slab bytes)
         self.completed: List[Job] = []
         self.launches = 0
         self.h2d_bytes = 0
@@ -73,6 +84,7 @@ class PersistentServer:
     def submit(self, rid: int, arrival: float, A, b, x0=None, kwargs: Optional[dict] = None) -> Job:
         """Validate a request on the host and queue it (``amen`` arguments)."""
         job = Job(rid, arrival, _Prepared(A, b, x0, dict(kwargs or {})), self.rmax)
+        job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
         self.queue.append(job)
         return job
 
@@ -83,6 +95,18 @@ class PersistentServer:
             return False
         rmax = min(j.rmax for j in self.queue)
         take = [j for j in self.queue if j.rmax == rmax][: self.max_batch]
+        if self.mem_budget is not None:
+            room = self.mem_budget - self.inflight_bytes
+            fit, used = [], 0
+            for j in take:  # arrival order: the oldest requests are admitted first
+                if used + j.slab_bytes <= room:
+                    fit.append(j)
+                    used += j.slab_bytes
+            if not fit and not self.inflight:
+                fit = take[:1]  # larger than the whole budget: alone
+            if not fit:
+                return False
+            take = fit
         taken = set(id(j) for j in take)
         self.queue = [j for j in self.queue if id(j) not in taken]
         take.sort(key=lambda j: -_cost(j.prep))
@@ -94,7 +118,10 @@ class PersistentServer:
             ev = torch.cuda.Event()
             ev.record(s)
         self.h2d_bytes += batch.h2d_bytes
-        self.inflight.append((si, batch, ev, take))
+        nbytes = sum(j.slab_bytes for j in take)
+        self.inflight_bytes += nbytes
+        self.peak_bytes = max(self.peak_bytes, self.inflight_bytes)
+        self.inflight.append((si, batch, ev, take, nbytes))
         self.launches += 1
         self._last_launch = now
         return True
@@ -102,16 +129,18 @@ class PersistentServer:
     def _collect(self, now: float) -> bool:
         done_any = False
         still = []
-        for si, batch, ev, jobs in self.inflight:
+        for si, batch, ev, jobs, nbytes in self.inflight:
             if not ev.query():
-                still.append((si, batch, ev, jobs))
+                still.append((si, batch, ev, jobs, nbytes))
                 continue
             done_any = True
+            self.inflight_bytes -= nbytes
             with torch.cuda.stream(self.streams[si]):
                 results = batch.collect()
                 for job, res in zip(jobs, results):
                     if res.status == -4 and job.rmax < self.max_rmax:
                         job.rmax = min(2 * job.rmax, self.max_rmax)
+                        job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
                         self.queue.append(job)
                         continue
                     job.result = res
@@ -120,6 +149,7 @@ class PersistentServer:
                         self.d2h_bytes += sum(c.nbytes for c in job.host_cores)
                     job.done_at = now
                     self.completed.append(job)
+            batch.release()
             self.free.append(si)
         self.inflight = still
         return done_any
