@@ -34,6 +34,25 @@ from . import kernels as K
 from .persistent import PersistentBatch, Result, _cost, _Prepared, slab_doubles
 
 
+def admit(sizes: Sequence[int], room: Optional[int], idle: bool) -> List[int]:
+    """Indices of the waiting requests (given oldest first, by work-area
+    bytes) that one launch takes under a device-memory budget: in arrival
+    order, each one whose bytes still fit in ``room`` beside those already
+    taken (``room`` None: no budget, all of them).  When none fits and
+    nothing is in flight (``idle``), the oldest is taken alone, so a request
+    larger than the whole budget still runs."""
+    if room is None:
+        return list(range(len(sizes)))
+    out, used = [], 0
+    for i, b in enumerate(sizes):
+        if used + b <= room:
+            out.append(i)
+            used += b
+    if not out and idle and sizes:
+        out = [0]
+    return out
+
+
 @dataclass
 class Job:
     rid: int
@@ -95,18 +114,11 @@ class PersistentServer:
             return False
         rmax = min(j.rmax for j in self.queue)
         take = [j for j in self.queue if j.rmax == rmax][: self.max_batch]
-        if self.mem_budget is not None:
-            room = self.mem_budget - self.inflight_bytes
-            fit, used = [], 0
-            for j in take:  # arrival order: the oldest requests are admitted first
-                if used + j.slab_bytes <= room:
-                    fit.append(j)
-                    used += j.slab_bytes
-            if not fit and not self.inflight:
-                fit = take[:1]  # larger than the whole budget: alone
-            if not fit:
-                return False
-            take = fit
+        room = None if self.mem_budget is None else self.mem_budget - self.inflight_bytes
+        idx = admit([j.slab_bytes for j in take], room, not self.inflight)
+        if not idx:
+            return False
+        take = [take[i] for i in idx]
         taken = set(id(j) for j in take)
         self.queue = [j for j in self.queue if id(j) not in taken]
         take.sort(key=lambda j: -_cost(j.prep))
