@@ -738,11 +738,18 @@ def config(args, reqs, engine="reference"):
                         "residual 1e-8",
             "requests_per_step": len(reqs), "mix": kinds, "engine": engine,
             "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
-            "l2": "inputs larger than L2 (two batches of slabs, tens of GB); 512 MB flush "
-                  "before the timed region",
-            "steps": "alternate between two device-resident copies of the batch on two "
-                     "streams, so one step's last solves overlap the next step's first",
-            "parallelism": f"replicas x{args.gpus}"}
+            "parallelism": f"replicas x{args.gpus}", **_timing_notes(engine)}
+
+
+def _timing_notes(engine):
+    if engine == "persistent":
+        return {"l2": "inputs larger than L2 (two batches of slabs, tens of GB); 512 MB flush "
+                      "before the timed region",
+                "steps": "alternate between two device-resident copies of the batch on two "
+                         "streams, so one step's last solves overlap the next step's first"}
+    if engine == "reference":
+        return {"host": "the CPU oracle on the host cores; no device memory involved"}
+    return {"l2": "flushed (512 MB write) before every timed step"}
 
 
 if __name__ == "__main__":
