@@ -132,3 +132,37 @@ def test_mals_errors(tt):
         tt.mals(b, b)
     with pytest.raises(tt.DimensionMismatch):
         tt.mals(A, tt.TensorTrain(P.random_tt([4] * 2, 2, seed=1)))
+
+
+def _dense_ttm(matrix, order):
+    return O.tt_svd(matrix.reshape([2] * 2 * order), error=0.0,
+                    physical_indexes=[(2, 2)] * order, ttm=True)
+
+
+def test_mals_reference_behaviours(tt):
+    """Systems the reference's MALS tests solve (``tests/test_mals.py:53-101``),
+    on the device: a Toeplitz system of size 256 in one sweep from a rank-5
+    ones or random guess (rank cap 10), and a dense random operator from the
+    default guess in two sweeps, each to 1e-7 in solution and residual."""
+    import scipy.linalg as sla
+
+    order, size = 8, 256
+    mat = sla.toeplitz(np.arange(1, size + 1), np.arange(1, size + 1)).astype(float)
+    A = _dense_ttm(mat, order)
+    ref = np.linalg.solve(mat, np.ones(size))
+    for x0 in (tt.ones([2] * order, ranks=5).orthonormalize("right"),
+               tt.TensorTrain(P.random_tt([2] * order, 5, 153))):
+        x = tt.mals(tt.TensorTrain(A.cores), tt.ones([2] * order), x0=x0, error_threshold=1e-7,
+                    max_rank=10, max_sweeps=1)
+        v = O.Train(x.to_numpy()).full().reshape(-1)
+        assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < 1e-7
+        assert O.relative_residual(A, O.ones([2] * order), O.Train(x.to_numpy())) < 1e-7
+    mat = np.random.default_rng(31).random((size, size))
+    A = _dense_ttm(mat, order)
+    ref = np.linalg.solve(mat, np.ones(size))
+    b = O.tt_svd((mat @ ref).reshape([2] * order), error=0.0)
+    x = tt.mals(tt.TensorTrain(A.cores), tt.TensorTrain(b.cores), error_threshold=1e-7,
+                max_sweeps=2)
+    v = O.Train(x.to_numpy()).full().reshape(-1)
+    assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < 1e-7
+    assert O.relative_residual(A, b, O.Train(x.to_numpy())) < 1e-7

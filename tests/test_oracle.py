@@ -272,3 +272,61 @@ def test_oracle_multiply_matches_reference():
         assert out.bonds == ref.bonds, name
         assert all(np.allclose(x, y, rtol=1e-8, atol=1e-10) for x, y in zip(out.cores, ref.cores)), name
         assert out.orth_center == ref.orth_center, name
+
+
+def _dense_ttm(matrix, order):
+    return O.tt_svd(matrix.reshape([2] * 2 * order), error=0.0,
+                    physical_indexes=[(2, 2)] * order, ttm=True)
+
+
+def test_oracle_mals_solves_toeplitz_from_either_guess():
+    """MALS behaviour the reference's tests pin (``tests/test_mals.py:53-79``):
+    a symmetric Toeplitz system of size 256 solved to 1e-7 in one sweep from
+    a rank-5 ones or random guess with the rank capped at 10."""
+    import scipy.linalg as sla
+
+    order, size = 8, 256
+    mat = sla.toeplitz(np.arange(1, size + 1), np.arange(1, size + 1)).astype(float)
+    A = _dense_ttm(mat, order)
+    b = O.ones([2] * order)
+    ref = np.linalg.solve(mat, np.ones(size))
+    guesses = [O.orthonormalize(O.ones([2] * order, ranks=5), "right"),
+               O.Train(P.random_tt([2] * order, 5, 153))]
+    for x0 in guesses:
+        x, _ = O.mals(A, b, x0=x0, error_threshold=1e-7, max_rank=10, max_sweeps=1)
+        v = x.full().reshape(-1)
+        assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < 1e-7
+        assert O.relative_residual(A, b, x) < 1e-7
+
+
+def test_oracle_mals_nonsymmetric_default_guess():
+    """A dense random operator solved from the default guess in two sweeps
+    (``tests/test_mals.py:81-101``)."""
+    order, size = 8, 256
+    mat = np.random.default_rng(31).random((size, size))
+    A = _dense_ttm(mat, order)
+    ref = np.linalg.solve(mat, np.ones(size))
+    b = O.tt_svd((mat @ ref).reshape([2] * order), error=0.0)
+    x, _ = O.mals(A, b, error_threshold=1e-7, max_sweeps=2)
+    v = x.full().reshape(-1)
+    assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < 1e-7
+    assert O.relative_residual(A, b, x) < 1e-7
+
+
+def test_oracle_qtt_reference_behaviours():
+    """``tt_to_qtt`` behaviours the reference's tests pin
+    (``tests/test_tensor_train.py:473-536``): the error stays within
+    ``error * ||A||``, bonds floor at 1 under a huge error, and cores that
+    need no split (mode 2) or modes like 243 = 3^5 are handled."""
+    dense = np.random.default_rng(0).standard_normal((8, 8, 8))
+    t = O.tt_svd(dense)
+    for err in (3e-1, 1e-1, 1e-2, 1e-4):
+        q = O.tt_to_qtt(t, error=err)
+        assert np.linalg.norm(q.full().reshape(8, 8, 8) - dense) <= err * np.linalg.norm(dense)
+    t16 = O.Train(P.random_tt([16, 16], 4, 120))
+    assert O.tt_to_qtt(t16, error=1e2).bonds == [1] * 9
+    for modes, base, seed in (([2, 8], 2, 121), ([243, 3], 3, 122)):
+        t = O.Train(P.random_tt(modes, 2, seed))
+        q = O.tt_to_qtt(t, mode_size=base, error=1e-12)
+        assert all(c.shape[1] == base for c in q.cores)
+        assert np.allclose(q.full().reshape(-1), t.full().reshape(-1), rtol=1e-10, atol=1e-12)
