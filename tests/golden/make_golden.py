@@ -8,6 +8,7 @@ next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
     python tests/golden/make_golden.py mals     # the MALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
     python tests/golden/make_golden.py hadamard # element-wise products only
+    python tests/golden/make_golden.py canonical  # canonical_tt only
     python tests/golden/make_golden.py tt_svd   # TT-SVD only
     python tests/golden/make_golden.py tt_to_qtt  # quantisation only
 
@@ -220,6 +221,18 @@ def hadamard_cases() -> None:
     save("hadamard", data, {"cases": cases})
 
 
+def canonical_cases() -> None:
+    """canonical_tt (tensor_train.py:1390-1446): the full-rank train of
+    canonical basis products."""
+    data = {}
+    cases = []
+    for name, dims, rank in [("odd", [2, 3, 4], 3), ("even", [2, 2, 2, 2, 2, 2], 4),
+                             ("mixed", [3, 2, 2, 3, 5], 10)]:
+        pack(data, f"out_{name}", tt.canonical_tt(dims, rank))
+        cases.append([name, dims, rank])
+    save("canonical_tt", data, {"cases": cases})
+
+
 def tt_svd_cases() -> None:
     """tt_svd (tensor_train.py:1138-1247): the dense-to-TT builder."""
     data = {}
@@ -292,6 +305,9 @@ def tt_to_qtt_cases() -> None:
 def main() -> None:
     if "tt_to_qtt" in sys.argv[1:]:
         tt_to_qtt_cases()
+        return
+    if "canonical" in sys.argv[1:]:
+        canonical_cases()
         return
     if "hadamard" in sys.argv[1:]:
         hadamard_cases()
@@ -425,6 +441,7 @@ def main() -> None:
     mals_cases()
     randomized_cases()
     hadamard_cases()
+    canonical_cases()
     tt_svd_cases()
     tt_to_qtt_cases()
 

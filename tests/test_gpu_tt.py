@@ -346,3 +346,15 @@ def test_multiply_errors(tt):
         p.multiply(p, truncate=True, method="randomized", max_rank=0)
     with pytest.raises(TypeError):
         p.multiply("x")
+
+
+def test_canonical_tt_matches_reference(tt):
+    """``canonical_tt`` on the device: the reference's cores and centre."""
+    data = load_golden("canonical_tt")
+    for name, dims, rank in data["args"]["cases"]:
+        t = tt.canonical_tt(dims, rank)
+        ref_c, ref_oc = golden_train(data, f"out_{name}")
+        assert t.orth_center == ref_oc, name
+        assert all(np.array_equal(a, b) for a, b in zip(t.to_numpy(), ref_c)), name
+    with pytest.raises(tt.WrongTTFormat):
+        tt.canonical_tt([4], 2)

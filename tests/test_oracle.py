@@ -330,3 +330,17 @@ def test_oracle_qtt_reference_behaviours():
         q = O.tt_to_qtt(t, mode_size=base, error=1e-12)
         assert all(c.shape[1] == base for c in q.cores)
         assert np.allclose(q.full().reshape(-1), t.full().reshape(-1), rtol=1e-10, atol=1e-12)
+
+
+def test_canonical_cores_match_reference():
+    """``canonical_tt`` (``tensor_train.py:1390-1446``): the host cores the
+    device constructor uploads equal the reference's, with its centre."""
+    from ttnumpy_b200.tensor_train import canonical_cores
+
+    data = load_golden("canonical_tt")
+    for name, dims, rank in data["args"]["cases"]:
+        cores, center = canonical_cores(dims, rank)
+        ref = _train(data, f"out_{name}")
+        assert len(cores) == len(ref.cores), name
+        assert all(np.array_equal(a, b) for a, b in zip(cores, ref.cores)), name
+        assert center == ref.orth_center, name

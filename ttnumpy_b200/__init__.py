@@ -26,6 +26,7 @@ from .tensor_train import (  # noqa: F401
     TensorTrainType,
     WrongTTFormat,
     WrongTTType,
+    canonical_tt,
     eye,
     ones,
     rand,
@@ -36,5 +37,5 @@ from .tensor_train import (  # noqa: F401
 __all__ = [
     "TensorTrain", "TensorTrainType", "ones", "zeros", "eye", "rand", "amen", "als", "mals",
     "SolverInfo", "StopReason", "LocalSolver", "TruncationMode", "relative_residual",
-    "DimensionMismatch", "WrongTTFormat", "WrongTTType", "AmbiguousFormat", "tt_svd",
+    "DimensionMismatch", "WrongTTFormat", "WrongTTType", "AmbiguousFormat", "tt_svd", "canonical_tt",
 ]

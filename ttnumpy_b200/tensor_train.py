@@ -869,6 +869,38 @@ def eye(physical_indexes) -> TensorTrain:
     return TensorTrain([np.eye(p).reshape(1, p, p, 1) for p in physical_indexes])
 
 
+def canonical_cores(physical_indexes, max_rank: int) -> Tuple[List[np.ndarray], int]:
+    """Host cores of ``canonical_tt`` and its orthogonality centre
+    (``tensor_train.py:1390-1446``): products of canonical basis vectors,
+    bond k = min(max_rank, states left of the cut, states right of it); the
+    first half of the cores is left-orthogonal (the identity on the
+    (bond, mode) -> bond unfolding), the rest right-orthogonal, and for an
+    odd number of cores the middle one is left-orthogonal."""
+    dims = [int(p) for p in physical_indexes]
+    d = len(dims)
+    if d < 2:
+        raise WrongTTFormat("Tensor train must have at least two cores.")
+    bonds = [1] * (d + 1)
+    for k in range(1, d):
+        bonds[k] = min(max_rank, math.prod(dims[:k]), math.prod(dims[k:]))
+    half = d // 2
+    cores = []
+    for i, n in enumerate(dims):
+        if i < half + d % 2:  # left-orthogonal, the middle core of an odd train included
+            m = np.eye(bonds[i] * n, bonds[i + 1])
+        else:
+            m = np.eye(bonds[i], n * bonds[i + 1])
+        cores.append(m.reshape(bonds[i], n, 1, bonds[i + 1]))
+    return cores, (half if d % 2 else half - 1)
+
+
+def canonical_tt(physical_indexes, max_rank: int) -> TensorTrain:
+    """Full-rank train of canonical basis products, built on the host and
+    uploaded (``tensor_train.py:1390-1446``)."""
+    cores, center = canonical_cores(physical_indexes, max_rank)
+    return TensorTrain(cores, orth_center=center)
+
+
 def rand(physical_indexes, ranks=1, seed=None) -> TensorTrain:
     """Uniform [0, 1) cores from ``np.random.default_rng(seed)``, drawn core
     by core exactly as the reference does, then uploaded."""
