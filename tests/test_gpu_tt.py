@@ -358,3 +358,38 @@ def test_canonical_tt_matches_reference(tt):
         assert all(np.array_equal(a, b) for a, b in zip(t.to_numpy(), ref_c)), name
     with pytest.raises(tt.WrongTTFormat):
         tt.canonical_tt([4], 2)
+
+
+def test_element_matricize_transpose(tt):
+    """``get_element``, ``matricize``, ``transpose`` and ``conj``
+    (``tensor_train.py:556-703``) against the dense tensors of the host
+    cores, for a TT and a TTM (reference tests/test_tensor_train.py:60-145)."""
+    rng = np.random.default_rng(7)
+    ranks = [1, 2, 3, 1]
+    tcores = [rng.standard_normal((ranks[k], 3, 1, ranks[k + 1])) for k in range(3)]
+    mcores = [rng.standard_normal((ranks[k], 2, 3, ranks[k + 1])) for k in range(3)]
+    t, m = tt.TensorTrain(tcores), tt.TensorTrain(mcores)
+    vec_t = O.Train(tcores).full()  # the reference's matricize order
+    dense_t = vec_t.reshape(3, 3, 3)
+    assert t.get_element([2, 0, 1]) == pytest.approx(dense_t[2, 0, 1], rel=1e-13)
+    assert t.get_element([(1, 0), (2, 0), (0, 0)]) == pytest.approx(dense_t[1, 2, 0], rel=1e-13)
+    with pytest.raises(tt.DimensionMismatch):
+        t.get_element([0, 0])
+    np.testing.assert_allclose(t.matricize(), vec_t, rtol=1e-13, atol=1e-14)
+    # TTM: the (rows x columns) operator, entries indexed (rows..., cols...)
+    mat_m = O.Train(mcores).full()
+    dense_m = mat_m.reshape(2, 2, 2, 3, 3, 3)
+    assert m.get_element([(1, 2), (0, 0), (1, 1)]) == pytest.approx(dense_m[1, 0, 1, 2, 0, 1],
+                                                                   rel=1e-13)
+    np.testing.assert_allclose(m.matricize(), mat_m, rtol=1e-13, atol=1e-14)
+    mt = m.transpose()
+    assert mt.row_modes == [3, 3, 3] and mt.col_modes == [2, 2, 2]
+    np.testing.assert_allclose(mt.matricize(), mat_m.T, rtol=1e-13, atol=1e-14)
+    part = m.transpose([0])
+    assert np.array_equal(part.to_numpy()[0], mcores[0].transpose(0, 2, 1, 3))
+    assert np.array_equal(part.to_numpy()[1], mcores[1])
+    assert np.array_equal(m.to_numpy()[0], mcores[0])  # not in place
+    back = mt.transpose(conjugate=True).conj()
+    assert all(np.array_equal(a, b) for a, b in zip(back.to_numpy(), mcores))
+    col = t.transpose()
+    assert col.is_ttm() and col.col_modes == [3, 3, 3]

@@ -191,6 +191,52 @@ class TensorTrain:
             return t.item()
         return t.reshape(shape)
 
+    def get_element(self, element_index) -> float:
+        """One entry (``tensor_train.py:556-596``): the product of each
+        core's (bond x bond) slice at the given index, by device GEMMs on the
+        strided slices.  A TT takes plain indices, a TTM (row, column)
+        pairs."""
+        if len(element_index) != len(self):
+            raise DimensionMismatch(
+                "Number of indexes not equal to number of tensor train cores: "
+                f"{len(element_index)} != {len(self)}")
+        idx = list(element_index)
+        if self.tt_type is TensorTrainType.TT and isinstance(idx[0], (int, np.integer)):
+            idx = [(int(i), 0) for i in idx]
+        acc = self.cores[0][:, idx[0][0], idx[0][1], :]
+        for core, (i, j) in zip(self.cores[1:], idx[1:]):
+            acc = K.matmul(acc, core[:, i, j, :])
+        return acc.reshape(-1)[0].item()
+
+    def matricize(self):
+        """The train as a vector (TT) or a (rows x columns) matrix (TTM) on
+        the host (``tensor_train.py:626-638``), the cores merged on the
+        device first."""
+        merged = _merge_cores([c.contiguous() for c in self.cores]).cpu().numpy()
+        if not self.is_ttm():
+            return merged.reshape(-1)
+        return merged.reshape(math.prod(self.row_modes), math.prod(self.col_modes))
+
+    def transpose(self, cores_ind: Optional[List[int]] = None, conjugate: bool = False,
+                  inplace: bool = False) -> "TensorTrain":
+        """Swap the row and column modes of the given cores (all by default)
+        by one permuted copy each (``tensor_train.py:647-689``).  The cores
+        are real, so ``conjugate`` changes nothing."""
+        t = self if inplace else self.copy()
+        for i in (range(len(t)) if cores_ind is None else cores_ind):
+            c = t.cores[i]
+            out = K.empty(c.shape[0], c.shape[2], c.shape[1], c.shape[3])
+            K.copy_(out, c.permute(0, 2, 1, 3))
+            t.cores[i] = out
+        t.tt_type = (TensorTrainType.TT if all(c.shape[2] == 1 for c in t.cores)
+                     else TensorTrainType.TTM)
+        return t
+
+    def conj(self, inplace: bool = False) -> "TensorTrain":
+        """Complex conjugate (``tensor_train.py:691-703``): the cores are
+        real float64, so the train itself (or a copy)."""
+        return self if inplace else self.copy()
+
     # -- arithmetic ---------------------------------------------------------
 
     def add(self, other: "TensorTrain", truncate: bool = False, error=None, max_rank=None,
