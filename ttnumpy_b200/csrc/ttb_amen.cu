@@ -487,12 +487,14 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   const i64 mark = c.top;
   double* buf = take(c, 7 * N);
   if (c.status) return;
+  // r1, r2 and w, w2 rotate by pointer (SciPy's r1 <- r2, r2 <- y and
+  // w1 <- w2, w2 <- w copies); y is the operator's output, and after each
+  // iteration its value is r2's
   double* r1 = buf;
   double* r2 = buf + N;
   double* y = buf + 2 * N;
   double* v = buf + 3 * N;
   double* w = buf + 4 * N;
-  double* w1 = buf + 5 * N;
   double* w2 = buf + 6 * N;
   if (warm) {
     apply(c, L, x, y, 1, 1.0, 0.0);
@@ -521,24 +523,34 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   int istop = 0;
   for (int itn = 1; itn <= maxit; ++itn) {
     const double s = 1.0 / beta;
-    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) v[i] = s * y[i];
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) v[i] = s * r2[i];
     __syncthreads();
     apply(c, L, v, y, 1, 1.0, 0.0);
     if (c.status) return;
+    // y -= (beta / oldb) r1 and alfa = v . y in one pass
+    double dot = 0.0;
     if (itn >= 2) {
       const double f = beta / oldb;
-      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) y[i] -= f * r1[i];
-      __syncthreads();
+      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+        const double yi = y[i] - f * r1[i];
+        y[i] = yi;
+        dot = fma(v[i], yi, dot);
+      }
+    } else {
+      for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) dot = fma(v[i], y[i], dot);
     }
-    const double alfa = vdot(v, y, N, red);
+    const double alfa = block_sum(dot, red);
     const double g = alfa / beta;
     double part = 0.0;
     for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
-      double yi = y[i] - g * r2[i];
-      r1[i] = r2[i];
-      r2[i] = yi;
-      y[i] = yi;
+      const double yi = y[i] - g * r2[i];
+      r1[i] = yi;  // the new r2; r1 was last read above
       part = fma(yi, yi, part);
+    }
+    {
+      double* t = r1;
+      r1 = r2;
+      r2 = t;
     }
     oldb = beta;
     beta = sqrt(block_sum(part, red));
@@ -560,12 +572,15 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
       double a1 = w2[i], a2 = w[i];
       double wn = (v[i] - oldeps * a1 - delta * a2) * denom;
-      w1[i] = a1;
-      w2[i] = a2;
-      w[i] = wn;
+      w2[i] = wn;  // the new w; the old w becomes w2
       double xi = x[i] + phi * wn;
       x[i] = xi;
       xs = fma(xi, xi, xs);
+    }
+    {
+      double* t = w2;
+      w2 = w;
+      w = t;
     }
     gmax = fmax(gmax, gamma);
     gmin = fmin(gmin, gamma);
