@@ -964,31 +964,17 @@ def local_rhs_pair(left_b, b1, b2, right_b) -> np.ndarray:
 
 
 def local_matrix_pair(left_A, A1, A2, right_A) -> np.ndarray:
-    """Explicit two-site operator (``solvers/two_site.py:52-79``): rows
-    (frame bond, row k, row k+1, frame bond), columns the target side."""
-    t = np.einsum("iaj,aklb,bmnc,ocp->jkmpilno", left_A, A1, A2, right_A, optimize="optimal")
-    rows = left_A.shape[2] * A1.shape[1] * A2.shape[1] * right_A.shape[2]
-    return t.reshape(rows, -1)
+    """Explicit two-site operator (``solvers/two_site.py:52-79``): the
+    one-site operator of the merged core ``A1 A2`` (row modes and column
+    modes of the pair merged), which orders rows (frame bond, row k,
+    row k+1, frame bond) and columns likewise on the target side."""
+    return local_matrix(left_A, merge_cores([A1, A2]), right_A)
 
 
 def local_operator_pair(left_A, A1, A2, right_A):
     """Matrix-free two-site operator (``solvers/two_site.py:82-127``): the
-    right environment, the two operator cores and the left environment are
-    contracted into the block one after the other."""
-    shape = (left_A.shape[0], A1.shape[2], A2.shape[2], right_A.shape[0])
-    size = int(np.prod(shape))
-
-    def matmat(block):
-        y = np.asarray(block).reshape(shape + (-1,))
-        t = np.tensordot(y, right_A, axes=(3, 0))                 # (i, l, n, z, c, p)
-        t = np.tensordot(t, A2, axes=((2, 4), (2, 3)))           # (i, l, z, p, b, m)
-        t = np.tensordot(t, A1, axes=((1, 4), (2, 3)))           # (i, z, p, m, a, k)
-        t = np.tensordot(t, left_A, axes=((0, 4), (0, 1)))       # (z, p, m, k, j)
-        return t.transpose(4, 3, 2, 1, 0).reshape(size, -1)
-
-    return spla.LinearOperator(
-        (size, size), matvec=lambda v: matmat(v).ravel(), matmat=matmat, dtype=np.float64
-    )
+    matrix-free one-site operator of the merged core ``A1 A2``."""
+    return local_operator(left_A, merge_cores([A1, A2]), right_A)
 
 
 def _pair_warm_start(x: Train, k: int, center):

@@ -94,7 +94,8 @@ def test_oracle_mals_matches_reference(case):
     assert x.bonds == list(data["bonds"])
     assert info.max_bonds == list(data["max_bonds"])
     assert info.local_solves == int(data["local_solves"])
-    np.testing.assert_allclose(info.residuals, data["residuals"], rtol=1e-6, atol=1e-14)
+    # residuals at round-off level (below 1e-12) agree only to that level
+    np.testing.assert_allclose(info.residuals, data["residuals"], rtol=1e-6, atol=1e-12)
     diff = O.tt_norm(O.add(x, O.scale(ref_x, -1.0))) / O.tt_norm(ref_x)
     assert diff <= 1e-9
 
