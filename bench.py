@@ -372,14 +372,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0's host cores alone
     reqs = make_requests(args.requests, args.seed, _ints(args.diffusion_dims),
                          _ints(args.diffusion_modes))
     cores = cpu_cores()
     n_sample = args.cpu_sample or min(len(reqs), max(2 * cores, 8))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
         sample = cpu_sample(reqs, n_sample)
         for _ in range(args.warmup):
             cpu_run(sample[: min(len(sample), cores)], cores)
