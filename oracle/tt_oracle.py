@@ -2,7 +2,9 @@
 
 TEST INFRASTRUCTURE ONLY.  This module is a plain NumPy/SciPy restatement of
 the reference algorithm (ttnumpy 0.3.0): the AMEn one-site sweep, the TT
-rounding it depends on and the TTM-by-TT product.  It exists so that the
+rounding it depends on and the TTM-by-TT product, and beside them ALS, MALS,
+randomized rounding (generic and HaTT-1 for element-wise products), TT-SVD
+and the QTT conversions.  It exists so that the
 parity tests, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of
 ``bench.py`` have something to check the CUDA path against and something to
 time on the host cores.  Nothing in the product package imports it.
