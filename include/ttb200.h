@@ -198,7 +198,10 @@ int ttb_qr(const ttb_qr_t* problems, int count, void* stream);
  * (on different streams or host threads) race and must be serialised by the
  * caller.  The first call on each device, made with that device current,
  * looks up the array's address (count = 0 is enough); make it before any
- * stream capture begins on that device. */
+ * stream capture begins on that device.  The address is kept for the life
+ * of the process: after the caller resets a device (cudaDeviceReset) the
+ * kept address is stale, so do not call ttb_qr_static on that device
+ * again. */
 #define TTB_QR_STATIC_DOUBLES 2097152
 #define TTB_ERR_STATIC_SCRATCH (-2)
 int ttb_qr_static(const ttb_qr_t* problems, int count, void* stream);
@@ -445,8 +448,9 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * ``slab`` (ttb_amen_slab_doubles() doubles); x bonds are capped at
  * ``rmax`` (status -4 when a bond would exceed it).  Results: result[0]
  * status (0 ok, -1 singular local system, -3 slab too small, -4 rank cap,
- * -5 unsupported settings), result[1] sweeps run, result[2] stop reason
- * (0 converged, 1 stagnated, 2 max sweeps), result[3] local solves,
+ * -5 unsupported settings, -6 time limit), result[1] sweeps run,
+ * result[2] stop reason (0 converged, 1 stagnated, 2 max sweeps),
+ * result[3] local solves,
  * result[4] inexact local solves, result[5..5+d] x bonds;
  * residuals[0..sweeps-1] and, from residuals[max_sweeps], the largest
  * bond after each sweep; residuals[2 * max_sweeps] receives the FP64 FLOPs
@@ -488,6 +492,12 @@ typedef struct {
                 repeat every two-level R-only QR with the one-level one and
                 record the worst relative gap of R in [2*max_sweeps + 12],
                 the number of such QRs in [+ 13] */
+  long long time_limit_ns; /* > 0: the solve stops with status -6 after the
+                              first local step that ends this many ns of the
+                              device timer after the block started (the
+                              per-solve time limit of the reference's
+                              benchmark runner, benchmarks/poisson.py:95-143);
+                              sweeps, residuals and bonds so far are kept */
 } ttb_amen_task_t;
 long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int rmax,
                                 int direct_solve_size);

@@ -1,9 +1,9 @@
 """Generate the golden fixtures by running the reference package itself.
 
-Run from the repository root, in a checkout that has the reference project
-next to it (the default path below, or ``TTNUMPY_REFERENCE``)::
+Run from the repository root with ``TTNUMPY_REFERENCE`` set to the
+reference checkout (the directory holding the ``ttnumpy`` package)::
 
-    python tests/golden/make_golden.py          # every case
+    TTNUMPY_REFERENCE=<checkout> python tests/golden/make_golden.py  # every case
     python tests/golden/make_golden.py als      # the ALS cases only
     python tests/golden/make_golden.py mals     # the MALS cases only
     python tests/golden/make_golden.py randomized  # randomized rounding only
@@ -33,7 +33,11 @@ import numpy as np  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("TTNUMPY_REFERENCE", "/root/reference")
+# the reference checkout (the directory holding the ``ttnumpy`` package)
+REFERENCE = os.environ.get("TTNUMPY_REFERENCE")
+if not REFERENCE or not os.path.isdir(os.path.join(REFERENCE, "ttnumpy")):
+    sys.exit("make_golden.py: set TTNUMPY_REFERENCE to the reference checkout "
+             "(the directory that holds the ttnumpy package)")
 sys.path.insert(0, REFERENCE)
 sys.path.insert(0, ROOT)
 

@@ -1,7 +1,8 @@
 """The serving loop's admission rule by device memory (host logic, no GPU):
-oldest requests first, each while the launch's work areas fit in the room
-the launches in flight leave; a request larger than the whole budget runs
-alone once nothing else is in flight."""
+the oldest requests, in arrival order, while the launch's work areas fit in
+the room the launches in flight leave; the first one that does not fit
+stops the launch (no younger request overtakes it); a request larger than
+the whole budget runs alone once nothing else is in flight."""
 
 from ttnumpy_b200.persistent_serving import admit
 
@@ -13,8 +14,10 @@ def test_no_budget_takes_everything():
 
 def test_oldest_first_while_they_fit():
     assert admit([3, 4, 5], 8, idle=False) == [0, 1]
-    # a large request does not block smaller, younger ones behind it
-    assert admit([3, 6, 2], 6, idle=False) == [0, 2]
+    # a large request that does not fit yet holds back the younger ones
+    # behind it, so it cannot be overtaken indefinitely
+    assert admit([3, 6, 2], 6, idle=False) == [0]
+    assert admit([6, 2], 6, idle=False) == [0]
     assert admit([2, 2, 2, 2], 8, idle=True) == [0, 1, 2, 3]
 
 

@@ -101,7 +101,8 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // shared memory the one-CTA factorisations may use (B200: 227 KB per block)
 constexpr int kSmemCap = 200 * 1024;
 
-int g_smem_configured = 0;
+int g_smem_qr[kMaxDevices], g_smem_svd[kMaxDevices], g_smem_lu[kMaxDevices],
+    g_smem_round[kMaxDevices];
 
 // ---------------------------------------------------------------------------
 // grouped GEMM
@@ -441,12 +442,12 @@ __global__ void __launch_bounds__(TTB_THREADS) k_lu(const __grid_constant__ LBat
   if (q.info && threadIdx.x == 0) *q.info = info;
 }
 
-void configure_smem() {
-  if (g_smem_configured) return;
-  cudaFuncSetAttribute(k_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap);
-  cudaFuncSetAttribute(k_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap);
-  cudaFuncSetAttribute(k_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap);
-  g_smem_configured = 1;
+// the one-CTA factorisations' shared-memory limit on the current device
+int configure_smem() {
+  int e = smem_limit_once((const void*)k_qr, kSmemCap, g_smem_qr);
+  if (!e) e = smem_limit_once((const void*)k_svd, kSmemCap, g_smem_svd);
+  if (!e) e = smem_limit_once((const void*)k_lu, kSmemCap, g_smem_lu);
+  return e;
 }
 
 // ---------------------------------------------------------------------------
@@ -1364,6 +1365,18 @@ int qr_static_base(double** out) {
 
 namespace ttb {
 void count_launch() { counted(); }
+
+int smem_limit_once(const void* func, int bytes, int* done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+  if (__atomic_load_n(&done[dev], __ATOMIC_ACQUIRE)) return 0;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return (int)e;
+  __atomic_store_n(&done[dev], 1, __ATOMIC_RELEASE);
+  return 0;
+}
 }  // namespace ttb
 
 // ===========================================================================
@@ -1485,7 +1498,7 @@ int ttb_project(const ttb_project_t* ps, int count, void* stream) {
 long long ttb_qr_work_doubles(int m, int k) { return qr_need(m, k); }
 
 int ttb_qr(const ttb_qr_t* ps, int count, void* stream) {
-  configure_smem();
+  if (int e = configure_smem()) return e;
   cudaStream_t s = as_stream(stream);
   for (int i0 = 0; i0 < count; i0 += kMaxQ) {
     QBatch qb;
@@ -1565,7 +1578,7 @@ long long ttb_svd_work_doubles(int m, int k) {
 }
 
 int ttb_svd(const ttb_svd_t* ps, int count, void* stream) {
-  configure_smem();
+  if (int e = configure_smem()) return e;
   cudaStream_t s = as_stream(stream);
   for (int i0 = 0; i0 < count; i0 += kMaxS) {
     SBatch sb;
@@ -1600,7 +1613,7 @@ int ttb_svd(const ttb_svd_t* ps, int count, void* stream) {
 long long ttb_lu_work_doubles(int n) { return (long long)n * LNB; }
 
 int ttb_lu_solve(const ttb_lu_t* ps, int count, void* stream) {
-  configure_smem();
+  if (int e = configure_smem()) return e;
   cudaStream_t s = as_stream(stream);
   for (int i0 = 0; i0 < count; i0 += kMaxL) {
     LBatch lb;
@@ -1940,14 +1953,10 @@ long long ttb_round_work_doubles(int d, int max_mode, int max_bond) {
 int ttb_round_batch(const ttb_round_t* P, void* stream) {
   if (P->pairs <= 0) return 0;
   if (P->d < 2 || P->d > kRoundMaxD) return (int)cudaErrorInvalidValue;
-  static int configured = 0;
   const size_t smem = ((size_t)kRoundMaxRows * kRoundMaxBond + kRoundMaxBond +
                        2 * (size_t)kRoundMaxBond * kRoundMaxBond + 3 * kRoundMaxBond + 2) *
                       sizeof(double);
-  if (!configured) {
-    cudaFuncSetAttribute(k_round, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = 1;
-  }
+  if (int e = smem_limit_once((const void*)k_round, (int)smem, g_smem_round)) return e;
   const long long qslot = (long long)kRoundMaxRows * kRoundMaxBond;
   const long long slot = qslot;
   ProfScope ps(P_ROUND, as_stream(stream), 0.0, 0.0);

@@ -39,7 +39,7 @@ constexpr double kShrink = 1e-2;       // common.py:233
 constexpr int kMaxMinres = 2000;       // iteration cap of one MINRES call
 constexpr double kEps = 2.220446049250313e-16;
 
-enum { ST_OK = 0, ST_SINGULAR = -1, ST_SLAB = -3, ST_RANK = -4, ST_SETTINGS = -5 };
+enum { ST_OK = 0, ST_SINGULAR = -1, ST_SLAB = -3, ST_RANK = -4, ST_SETTINGS = -5, ST_TIME = -6 };
 enum { F_A = 0, F_B, F_ZB, F_ZAX, F_XZ };
 
 struct Sm {
@@ -485,7 +485,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
                        int maxit, bool warm) {
   double* red = c.sm->red;
   const i64 mark = c.top;
-  double* buf = take(c, 7 * N);
+  double* buf = take(c, 6 * N);
   if (c.status) return;
   // r1, r2 and w, w2 rotate by pointer (SciPy's r1 <- r2, r2 <- y and
   // w1 <- w2, w2 <- w copies); y is the operator's output, and after each
@@ -495,7 +495,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   double* y = buf + 2 * N;
   double* v = buf + 3 * N;
   double* w = buf + 4 * N;
-  double* w2 = buf + 6 * N;
+  double* w2 = buf + 5 * N;
   if (warm) {
     apply(c, L, x, y, 1, 1.0, 0.0);
     for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) r1[i] = b[i] - y[i];
@@ -1289,6 +1289,17 @@ __device__ __noinline__ double train_norm(Ctx& c, int which) {
   return 0.0;
 }
 
+// True on every thread once the solve has run past its time limit: thread 0
+// reads the device timer and the block follows its decision.
+__device__ __noinline__ bool over_time(Ctx& c, unsigned long long t_start) {
+  if (c.T->time_limit_ns <= 0) return false;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    c.sm->flag = (global_ns() - t_start > (unsigned long long)c.T->time_limit_ns) ? 1 : 0;
+  __syncthreads();
+  return c.sm->flag != 0;
+}
+
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
@@ -1386,10 +1397,15 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
   }
   __syncthreads();
   int nsolves = 0, ninexact = 0, sweeps = 0, stop = 2;
-#define CHECK                                  \
-  if (c.status) {                              \
-    if (threadIdx.x == 0) T->result[0] = c.status; \
-    return;                                    \
+#define CHECK                                                      \
+  if (c.status) {                                                  \
+    if (threadIdx.x == 0) {                                        \
+      T->result[0] = c.status;                                     \
+      T->result[1] = sweeps;                                       \
+      T->residuals[2 * T->max_sweeps + 10] = (double)t_start;      \
+      T->residuals[2 * T->max_sweeps + 11] = (double)global_ns();  \
+    }                                                              \
+    return;                                                        \
   }
   if (T->x0_orth_center != 0) orth_right(c, true, d - 1);
   CHECK;
@@ -1470,6 +1486,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
       CHECK;
       PHASE(PH_TRUNC);
       c.top = base;
+      if (over_time(c, t_start)) c.status = ST_TIME;
+      CHECK;
     }
     for (int f = 0; f < 5; ++f) build_env(c, 0, f, d - 1);
     CHECK;
@@ -1501,6 +1519,8 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
       }
       PHASE(PH_TRUNC);
       c.top = base;
+      if (over_time(c, t_start)) c.status = ST_TIME;
+      CHECK;
     }
     sweeps = sweep + 1;
     {
@@ -1594,7 +1614,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   const long long apply = 2 * r * n * R * r + R * n * n * R + R * r * r;  // + permute_op
   const long long dn = std::min<long long>(direct_solve_size, N);
   const long long direct = dn * dn + dn;
-  const long long iter = N + 7 * N + apply;
+  const long long iter = N + 6 * N + apply;
   const long long rank = 4 * N + 2LL * kRankChunk * R * n * r + R * r * r + r * r + apply;
   const long long fact = r * n * r + r + r * n * r        // U S Vh
                          + (r * n) * r + 2 * r * r + 4 * r  // svd work
@@ -1610,12 +1630,9 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
 
 int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream) {
   if (count <= 0) return 0;
-  static int configured = 0;
+  static int configured[kMaxDevices];
   const size_t smem = kRingBytes + kPoolBytes;
-  if (!configured) {
-    cudaFuncSetAttribute(k_amen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = 1;
-  }
+  if (int e = smem_limit_once((const void*)k_amen, (int)smem, configured)) return e;
   k_amen<<<count, TTB_THREADS, smem, reinterpret_cast<cudaStream_t>(stream)>>>(tasks, rmax);
   ttb::count_launch();
   return (int)cudaGetLastError();

@@ -22,6 +22,13 @@ namespace ttb {
 
 typedef long long i64;
 
+// Host side (ttb200.cu): raise ``func``'s dynamic shared-memory limit to
+// ``bytes`` on the current device the first time a launch there needs it.
+// ``done`` holds one flag per device index (kMaxDevices); a flag is set only
+// after cudaFuncSetAttribute succeeded, and its error is returned otherwise.
+constexpr int kMaxDevices = 64;
+int smem_limit_once(const void* func, int bytes, int* done);
+
 // ---------------------------------------------------------------------------
 // reductions
 // ---------------------------------------------------------------------------

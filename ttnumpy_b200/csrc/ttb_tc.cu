@@ -30,6 +30,9 @@
 
 namespace ttb {
 void count_launch();  // the library's launch counter (ttb200.cu)
+constexpr int kMaxDevices = 64;
+// per-device shared-memory limit set-up (ttb200.cu)
+int smem_limit_once(const void* func, int bytes, int* done);
 }
 
 namespace {
@@ -66,7 +69,7 @@ struct TcBatch {
   TcDesc d[kMaxTc];
 };
 
-int g_tc_configured[64] = {0};
+int g_tc_configured[ttb::kMaxDevices];
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -285,15 +288,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_3xtf32(const __grid_constan
 extern "C" {
 
 int ttb_gemm_3xtf32(const ttb_gemm_t* ps, int count, int* status, void* stream) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return (int)e;
-  if (dev >= 0 && dev < 64 && !g_tc_configured[dev]) {
-    e = cudaFuncSetAttribute(k_gemm_3xtf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kSmemBytes);
-    if (e != cudaSuccess) return (int)e;
-    g_tc_configured[dev] = 1;
-  }
+  if (int e = ttb::smem_limit_once((const void*)k_gemm_3xtf32, (int)kSmemBytes, g_tc_configured))
+    return e;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int i = 0;
   while (i < count) {
@@ -331,7 +327,7 @@ int ttb_gemm_3xtf32(const ttb_gemm_t* ps, int count, int* status, void* stream) 
     if (blocks == 0) continue;
     k_gemm_3xtf32<<<blocks, THREADS, kSmemBytes, s>>>(tb, status);
     ttb::count_launch();
-    e = cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
   }
   return 0;

@@ -57,7 +57,7 @@ def _orth(t) -> Optional[int]:
 
 
 STATUS = {0: "ok", -1: "singular local system", -3: "slab too small", -4: "rank above rmax",
-          -5: "unsupported settings"}
+          -5: "unsupported settings", -6: "time limit"}
 
 
 @dataclass
@@ -149,7 +149,8 @@ class PersistentBatch:
     so a batch can be run again.
     """
 
-    def __init__(self, preps: List["_Prepared"], rmax: int, debug: bool = False):
+    def __init__(self, preps: List["_Prepared"], rmax: int, debug: bool = False,
+                 time_limit: Optional[float] = None):
         lib = _lib_handle()
         self.preps, self.rmax = preps, rmax
         n = len(preps)
@@ -216,6 +217,7 @@ class PersistentBatch:
                             else -1.0)
             t.truncation_tol = st.truncation_tol or 0.0
             t.debug = int(debug)
+            t.time_limit_ns = int(time_limit * 1e9) if time_limit else 0
         raw = np.frombuffer(bytes(tasks), dtype=np.uint8)
         self.dev_tasks = torch.from_numpy(raw.copy()).to("cuda")
 
@@ -272,6 +274,9 @@ class PersistentBatch:
         for i, p in enumerate(self.preps):
             status = int(res_h[i, 0])
             info = SolverInfo()
+            if status == -6:  # time limit: the sweeps completed before it
+                info.num_sweeps_run = int(res_h[i, 1])
+                info.residuals = [float(v) for v in resid_h[i, :info.num_sweeps_run]]
             if status != 0:
                 out.append(Result(None, info, status))
                 continue
@@ -328,15 +333,19 @@ def prepare(requests: Sequence) -> List["_Prepared"]:
 
 
 def amen_persistent(requests: Sequence, rmax: int = 64, max_rmax: int = 256,
-                    stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
+                    stream: Optional[torch.cuda.Stream] = None,
+                    time_limit: Optional[float] = None) -> List[Result]:
     """Solve ``[(A, b, x0, kwargs), ...]`` in one persistent launch; solves
-    whose bonds outgrow ``rmax`` are re-run with twice the capacity."""
+    whose bonds outgrow ``rmax`` are re-run with twice the capacity.  With
+    ``time_limit`` (seconds) a solve still running after that long on the
+    device stops with status -6."""
     K.device_ok()
     preps = prepare(requests)
     results: List[Optional[Result]] = [None] * len(preps)
     todo = list(range(len(preps)))
     while todo:
-        out = PersistentBatch([preps[i] for i in todo], rmax).run(stream)
+        out = PersistentBatch([preps[i] for i in todo], rmax,
+                              time_limit=time_limit).run(stream)
         retry = []
         for i, res in zip(todo, out):
             if res.status == -4 and rmax < max_rmax:

@@ -36,18 +36,21 @@ from .persistent import PersistentBatch, Result, _cost, _Prepared, slab_doubles
 
 def admit(sizes: Sequence[int], room: Optional[int], idle: bool) -> List[int]:
     """Indices of the waiting requests (given oldest first, by work-area
-    bytes) that one launch takes under a device-memory budget: in arrival
-    order, each one whose bytes still fit in ``room`` beside those already
-    taken (``room`` None: no budget, all of them).  When none fits and
-    nothing is in flight (``idle``), the oldest is taken alone, so a request
-    larger than the whole budget still runs."""
+    bytes) that one launch takes under a device-memory budget: the longest
+    prefix, in arrival order, whose bytes fit in ``room`` (``room`` None: no
+    budget, all of them).  The first request that does not fit stops the
+    launch, so later, smaller arrivals never overtake it and an old large
+    request cannot starve.  When none fits and nothing is in flight
+    (``idle``), the oldest is taken alone, so a request larger than the
+    whole budget still runs."""
     if room is None:
         return list(range(len(sizes)))
     out, used = [], 0
     for i, b in enumerate(sizes):
-        if used + b <= room:
-            out.append(i)
-            used += b
+        if used + b > room:
+            break
+        out.append(i)
+        used += b
     if not out and idle and sizes:
         out = [0]
     return out
