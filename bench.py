@@ -1,28 +1,41 @@
 #!/usr/bin/env python
 """AMEn solves/s and p50/p99 latency at relative residual 1e-8 on B200.
 
-One step = solving one batch of synthetic requests (a seeded mix of 2-D QTT
-Poisson problems with 6-20 cores and parametric diffusion problems with
-d in {4, 5}, n in {16, 32}), each to relative residual 1e-8.  The requests
-are identical in every step.  ``--engine plain`` solves them one at a time
-through the drop-in ``amen``; ``--engine served`` (the default once
-available) admits all of them into the batched serving engine.
+Workload (``--preset config5``, the default): the serving mix of requests,
+each drawn from one seeded generator (``problems.serving_request``): 10 %
+large diffusion solves (d = 24, n = 64, random rank-8 right-hand side), the
+rest in equal parts parametric diffusion (d ~ U{4..12}, n ~ U{16, 32, 64},
+theta ~ U(-1, 1)) and 2-D QTT Poisson problems with 6-20 cores.  Every
+request is solved to relative residual 1e-8 with at most 30 sweeps; a
+request that stops above the tolerance counts as not solved.  A step is one
+batch of ``--requests`` consecutive requests of the stream (every step a
+different batch).  ``--preset small`` is a reduced mix (diffusion d in
+{4, 5}, n in {16, 32}).
+
+``value``: the warm-up and timed steps' requests are uploaded to the device
+first; the timed steps' requests are then queued at once, longest first, to
+the continuous-batching server on the persistent whole-solve kernel
+(``persistent_serving``), and value = solved requests / device time of the
+whole run.  ``e2e``: the same server fed from host memory through its public
+API (inputs copied per launch, solutions read back) with a seeded Poisson
+stream arriving at twice the measured capacity; two more passes at 0.5x and
+0.8x of it report the latency at sustainable load.
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
-(the NumPy/SciPy restatement of the reference path) on the host cores
-instead, on a bounded sample of the same requests.
+(the NumPy/SciPy restatement of the reference path, kept within a few
+percent of the reference's own speed) on the host cores instead, on bounded
+samples of the same stream.
 
 Launch: ``python bench.py`` (1 GPU) or, for N GPUs,
 ``python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N``:
-every rank serves its own copy of the request batch (replicas; independent
-solves need no collective), ``value`` = all ranks' solves / max time.
+every rank serves its own copy of the stream (replicas; independent solves
+need no collective), ``value`` = all ranks' solves / max time.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import multiprocessing as mp
 import os
 import statistics
@@ -40,34 +53,38 @@ METRIC = "AMEn solves/s at relative residual 1e-8"
 UNIT = "solves/s"
 TOL = 1e-8
 MAX_SWEEPS = 30
+KINDS = ("qtt", "diffusion", "large")
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--engine", default="persistent", choices=["plain", "served", "persistent"])
-    ap.add_argument("--requests", type=int, default=1184,
-                    help="requests per step (1184 = 8 per SM of a B200)")
+    ap.add_argument("--preset", default="config5", choices=["config5", "small"])
+    ap.add_argument("--requests", type=int, default=148,
+                    help="requests per step (148 = one per SM of a B200)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-sample", type=int, default=0,
-                    help="requests in the CPU baseline sample (0: automatic)")
-    ap.add_argument("--serve-requests", type=int, default=0,
-                    help="requests in the served stream (0: three times --requests, the "
-                         "batch's requests cycled)")
-    ap.add_argument("--serve-mem-gb", type=float, default=48.0,
-                    help="device memory the server may hold in slabs of requests in flight")
-    ap.add_argument("--serve-rate", type=float, default=0.0,
-                    help="arrival rate of the served run (0: twice the measured batch rate)")
-    ap.add_argument("--plain-sample", type=int, default=8,
+    ap.add_argument("--serve-requests", type=int, default=600,
+                    help="requests in each served pass (a slice of the stream after the "
+                         "timed steps' requests)")
+    ap.add_argument("--serve-loads", default="0.5,0.8",
+                    help="arrival rates of the latency passes, as fractions of the measured "
+                         "capacity (the throughput pass arrives at twice it)")
+    ap.add_argument("--serve-mem-gb", type=float, default=96.0,
+                    help="device memory the server may hold in work areas of requests in flight")
+    ap.add_argument("--streams", type=int, default=32, help="server launch streams")
+    ap.add_argument("--max-batch", type=int, default=8, help="requests per server launch")
+    ap.add_argument("--plain-sample", type=int, default=64,
                     help="requests timed through the plain one-at-a-time drop-in (0: skip)")
-    ap.add_argument("--diffusion-dims", default="4,5",
-                    help="dimensions d the diffusion requests draw from")
-    ap.add_argument("--diffusion-modes", default="16,32",
-                    help="mode sizes n the diffusion requests draw from")
-    return ap.parse_args()
+    ap.add_argument("--plain-limit", type=float, default=2.0,
+                    help="per-solve time limit (s) of the plain drop-in sample")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="requests in the CPU baseline sample (0: two per host core)")
+    ap.add_argument("--cpu-limit", type=float, default=30.0,
+                    help="per-solve time limit (s) of the CPU oracle solves")
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------
@@ -75,39 +92,40 @@ def parse():
 # ---------------------------------------------------------------------------
 
 
-def make_requests(count: int, seed: int, dims=(4, 5), modes=(16, 32)):
-    """Seeded request mix: half 2-D QTT Poisson (N ~ U{3..10}, sin*sin
-    right-hand side), half parametric diffusion (d ~ U(dims), n ~ U(modes),
-    theta ~ U(-1, 1))."""
+def make_requests(count: int, seed: int, preset: str = "config5"):
+    """The first ``count`` requests of the seeded stream."""
     from ttnumpy_b200 import problems as P
 
-    rng = np.random.default_rng(seed)
-    dims, modes = tuple(dims), tuple(modes)
-    reqs = []
-    for i in range(count):
-        if i % 2 == 0:
-            N = int(rng.integers(3, 11))
-            p = P.qtt_poisson_2d(N)
-            p.meta["kind"] = "qtt"
-        else:
-            d = int(dims[int(rng.integers(0, len(dims)))])
-            n = int(rng.choice(modes))
-            p = P.parametric_diffusion(d, n, rng.uniform(-1.0, 1.0, size=d))
-            p.meta["kind"] = "diffusion"
-        reqs.append(p)
-    return reqs
+    if preset == "config5":
+        return P.serving_requests(count, seed)
+    return P.serving_requests(count, seed, large_share=0.0, dims=(4, 5), modes=(16, 32))
 
 
-# DRAM bytes (read + write) of one k_amen launch of the standard mix at
-# 1184 and 592 requests per step, from ncu captures of `python bench.py`
-# (profiles/k_amen_bench_*req.md); other workloads report null
-MEASURED_TRAFFIC = {1184: 1658012785152 + 1601813339392, 592: 655255445760 + 720370022144}
+def solve_kwargs(p):
+    return dict(residual_tol=TOL, symmetric=True, max_sweeps=MAX_SWEEPS, seed=0,
+                stagnation_factor=None)
 
 
-def _traffic(args):
-    standard = (args.seed == 0 and _ints(args.diffusion_dims) == [4, 5]
-                and _ints(args.diffusion_modes) == [16, 32])
-    return MEASURED_TRAFFIC.get(args.requests) if standard else None
+def x0_cores(p):
+    """Initial guess: rank-3 all-ones for QTT Poisson (the reference
+    benchmark's choice), the default (all-ones with b's ranks) otherwise."""
+    if p.meta.get("kind") == "qtt":
+        return 3
+    return None
+
+
+def x0_host(p):
+    r = x0_cores(p)
+    if r is None:
+        return None
+    modes = [c.shape[1] for c in p.b]
+    ranks = [1] + [r] * (len(modes) - 1) + [1]
+    return [np.ones((ranks[i], modes[i], 1, ranks[i + 1])) for i in range(len(modes))]
+
+
+def host_request(p):
+    """(A, b, x0, kwargs) as the server's public ``serve`` takes it."""
+    return (p.A, p.b, x0_host(p), solve_kwargs(p))
 
 
 def aggregate_rate(solved: int, ms: float, world: int, device: str = "cuda"):
@@ -126,21 +144,19 @@ def aggregate_rate(solved: int, ms: float, world: int, device: str = "cuda"):
     return solved / (ms * 1e-3), ms
 
 
-def _ints(text):
-    return [int(v) for v in str(text).split(",") if v.strip()]
-
-
-def solve_kwargs(p):
-    return dict(residual_tol=TOL, symmetric=True, max_sweeps=MAX_SWEEPS, seed=0,
-                stagnation_factor=None)
-
-
-def x0_cores(p):
-    """Initial guess: rank-3 all-ones for QTT Poisson (the reference
-    benchmark's choice), the default (all-ones with b's ranks) otherwise."""
-    if p.meta.get("kind") == "qtt":
-        return 3
-    return None
+def class_stats(kinds, solved, seconds=None):
+    """Per request class: requests, solved, and (with per-request
+    ``seconds``) their mean."""
+    out = {}
+    for k in KINDS:
+        idx = [i for i, kk in enumerate(kinds) if kk == k]
+        if not idx:
+            continue
+        row = {"requests": len(idx), "solved": int(sum(bool(solved[i]) for i in idx))}
+        if seconds is not None:
+            row["mean_s"] = float(np.mean([seconds[i] for i in idx]))
+        out[k] = row
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -148,7 +164,8 @@ def x0_cores(p):
 # ---------------------------------------------------------------------------
 
 
-def _cpu_solve(p):
+def _cpu_solve(args):
+    p, limit = args
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     from threadpoolctl import threadpool_limits
 
@@ -161,18 +178,19 @@ def _cpu_solve(p):
         if r is not None:
             x0 = O.orthonormalize(O.ones(b.row_modes, ranks=r), "right")
         t0 = time.perf_counter()
-        x, info = O.amen(A, b, x0=x0, **solve_kwargs(p))
+        x, info = O.amen(A, b, x0=x0, time_limit=limit, **solve_kwargs(p))
         dt = time.perf_counter() - t0
-    return dt, info.stop_reason, (info.residuals[-1] if info.residuals else float("nan"))
+    return dt, str(info.stop_reason) == "converged", p.meta.get("kind")
 
 
-def cpu_run(reqs, workers: int):
-    """Solve ``reqs`` on a spawn pool of single-threaded workers; returns
-    (seconds, per-request results)."""
+def cpu_run(reqs, workers: int, limit: float):
+    """Solve ``reqs`` on a spawn pool of single-threaded workers, each solve
+    capped at ``limit`` seconds; returns (wall seconds, per-request
+    (seconds, converged, class))."""
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(workers) as pool:
-        res = pool.map(_cpu_solve, reqs, chunksize=1)
+        res = pool.map(_cpu_solve, [(p, limit) for p in reqs], chunksize=1)
     return time.perf_counter() - t0, res
 
 
@@ -183,9 +201,21 @@ def cpu_cores() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_sample(reqs, n):
-    # every other request is QTT, so a prefix keeps the mix
-    return reqs[: max(2, n)]
+def cpu_baseline(reqs, cores, limit):
+    """CPU rate on a sample of the stream: solved requests over the CPU
+    time they took divided by the cores (the pool's sustained rate, not
+    bound by its slowest worker); capped solves count as unsolved at the
+    cap's time, which can only favour the CPU."""
+    wall, res = cpu_run(reqs, cores, limit)
+    cpu_s = sum(r[0] for r in res)
+    solved = sum(1 for r in res if r[1])
+    kinds = [r[2] for r in res]
+    return {"value": solved / (cpu_s / cores), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"the first {len(reqs)} requests of the stream, {cores} single-threaded "
+                      f"oracle workers, each solve capped at {limit:g} s; value = solved / "
+                      f"(sum of solve seconds / cores)",
+            "wall_s": wall, "cpu_s": cpu_s,
+            "classes": class_stats(kinds, [r[1] for r in res], [r[0] for r in res])}
 
 
 # ---------------------------------------------------------------------------
@@ -253,14 +283,6 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 
-def peaks():
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-            return json.load(fh)
-    except OSError:
-        return {}
-
-
 def fp64_peak_tflops(K, torch):
     """Measured FP64 FMA throughput of this GPU (own probe kernel)."""
     out = torch.zeros(1, dtype=torch.float64, device="cuda")
@@ -281,90 +303,97 @@ def fp64_peak_tflops(K, torch):
     return best
 
 
-class Engine:
-    """Solves a list of requests; returns results and per-request latencies (ms).
-
-    ``plain``: one drop-in ``amen`` call after another; ``served``: the
-    lockstep batch engine; ``persistent``: one persistent launch in which
-    every request is a thread block running its whole solve.
-    """
-
-    RMAX = 64
-
-    def __init__(self, kind: str):
-        import torch
-
-        import ttnumpy_b200 as tt
-
-        self.kind = kind
-        self.tt = tt
-        self.torch = torch
-
-    def upload(self, reqs):
-        """Inputs made resident on the device (not timed)."""
-        tt = self.tt
-        if self.kind == "persistent":
-            from ttnumpy_b200.persistent import PersistentBatch, prepare
-
-            return PersistentBatch(prepare([(p.A, p.b, self.x0_host(p), solve_kwargs(p))
-                                            for p in reqs]), self.RMAX)
-        out = []
-        for p in reqs:
-            A, b = tt.TensorTrain(p.A), tt.TensorTrain(p.b)
-            r = x0_cores(p)
-            x0 = tt.ones(b.physical_dims(), ranks=r).orthonormalize("right") if r else None
-            out.append((A, b, x0, p))
-        return out
-
-    @staticmethod
-    def x0_host(p):
-        r = x0_cores(p)
-        if r is None:
-            return None
-        modes = [c.shape[1] for c in p.b]
-        ranks = [1] + [r] * (len(modes) - 1) + [1]
-        return [np.ones((ranks[i], modes[i], 1, ranks[i + 1])) for i in range(len(modes))]
-
-    def solve_all(self, handle, download: bool = False):
-        torch = self.torch
-        if self.kind == "persistent":
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            handle.launch()
-            e.record()
-            res = handle.collect()
-            ms = s.elapsed_time(e)
-            for r in res:
-                if r.status != 0:
-                    raise RuntimeError(f"persistent solve failed with status {r.status}")
-            results = [(r.x, r.info) for r in res]
-            if download:
-                for x, _ in results:
-                    x.to_numpy()
-            return results, handle.latencies_ms()
-        lat = []
-        results = []
-        if self.kind == "plain":
-            for A, b, x0, p in handle:
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record()
-                x, info = self.tt.amen(A, b, x0=x0, return_info=True, **solve_kwargs(p))
-                if download:
-                    x.to_numpy()
-                e.record()
-                results.append((x, info))
-                lat.append((s, e))
-            torch.cuda.synchronize()
-            return results, [s.elapsed_time(e) for s, e in lat]
-        from ttnumpy_b200.serving import serve_batch
-
-        return serve_batch(handle, solve_kwargs, download=download)
+def _solved(job) -> bool:
+    r = job.result
+    return r is not None and r.status == 0 and bool(r.info.converged)
 
 
-def flush_l2(torch, buf):
+def make_server(args, resident: bool, download: bool):
+    from ttnumpy_b200.persistent_serving import PersistentServer
+
+    return PersistentServer(streams=args.streams, max_batch=args.max_batch,
+                            mem_budget=int(args.serve_mem_gb * 2**30), resident=resident,
+                            download=download)
+
+
+def resident_run(args, preps, torch):
+    """Closed-loop run of the server over device-resident requests, all
+    queued at once, longest first.  Returns (device ms, jobs, launches)."""
     from ttnumpy_b200 import kernels as K
+    from ttnumpy_b200.persistent import _cost
 
-    K.fill_(buf, 0.0)
+    order = sorted(range(len(preps)), key=lambda i: -_cost(preps[i]))
+    server = make_server(args, resident=True, download=False)
+    torch.cuda.synchronize()
+    l0 = K.launch_count()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    jobs = server.serve([preps[i] for i in order], [0.0] * len(order))
+    e.record()
+    torch.cuda.synchronize()
+    back = [None] * len(preps)
+    for j, i in enumerate(order):
+        back[i] = jobs[j]
+    return s.elapsed_time(e), back, K.launch_count() - l0, server
+
+
+def served_pass(args, reqs, rate, torch, seed):
+    """One pass of the server through its public API: host requests
+    arriving as a seeded Poisson stream at ``rate`` per second, inputs
+    copied per launch, solutions read back.  Timed with CUDA events around
+    the whole stream."""
+    host = [host_request(p) for p in reqs]
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(host)))
+    arrivals -= arrivals[0]
+    server = make_server(args, resident=False, download=True)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    jobs = server.serve(host, list(arrivals))
+    torch.cuda.synchronize()
+    e.record()
+    e.synchronize()
+    seconds = s.elapsed_time(e) * 1e-3
+    solved = sum(1 for j in jobs if _solved(j))
+    lats = [1e3 * j.latency for j in jobs if j.latency is not None]
+    out = {"rate": rate, "requests": len(jobs), "solved": solved, "seconds": seconds,
+           "throughput": solved / seconds,
+           "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
+           "h2d": server.h2d_bytes, "d2h": server.d2h_bytes, "launches": server.launches,
+           "peak_gb": server.peak_bytes / 2**30}
+    jobs = server = None
+    torch.cuda.empty_cache()
+    return out
+
+
+def plain_run(reqs, limit, torch):
+    """The plain one-solve-at-a-time FP64 GPU AMEn (the drop-in ``amen``,
+    every contraction and factorisation a library call) on the first
+    requests of the stream, each solve capped at ``limit`` seconds."""
+    import ttnumpy_b200 as tt
+    from ttnumpy_b200.solvers.amen import solve_time_limit
+
+    def one(p):
+        A, b = tt.TensorTrain(p.A), tt.TensorTrain(p.b)
+        r = x0_cores(p)
+        x0 = tt.ones(b.physical_dims(), ranks=r).orthonormalize("right") if r else None
+        with solve_time_limit(limit):
+            x, info = tt.amen(A, b, x0=x0, return_info=True, **solve_kwargs(p))
+        return bool(info.converged)
+
+    one(reqs[0])  # warm-up
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    ok = [one(p) for p in reqs]
+    e.record()
+    torch.cuda.synchronize()
+    kinds = [p.meta["kind"] for p in reqs]
+    return {"value": sum(ok) / (s.elapsed_time(e) * 1e-3), "unit": UNIT,
+            "sample": f"the first {len(reqs)} requests of the stream, solved one after another "
+                      f"by the drop-in amen, each capped at {limit:g} s",
+            "classes": class_stats(kinds, ok)}
 
 
 def main():
@@ -372,36 +401,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference" and rank != 0:
-        return  # the reference arm runs on rank 0's host cores alone
-    reqs = make_requests(args.requests, args.seed, _ints(args.diffusion_dims),
-                         _ints(args.diffusion_modes))
-    cores = cpu_cores()
-    n_sample = args.cpu_sample or min(len(reqs), max(2 * cores, 8))
-
     if args.impl == "reference":
-        sample = cpu_sample(reqs, n_sample)
-        for _ in range(args.warmup):
-            cpu_run(sample[: min(len(sample), cores)], cores)
-        total, n = 0.0, 0
-        for _ in range(args.steps):
-            dt, res = cpu_run(sample, cores)
-            total += dt
-            n += sum(1 for r in res if str(r[1]) == "converged")
-        value = n / total
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config(args, reqs),
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                                 "sample": f"{len(sample)} of the {len(reqs)} requests per step "
-                                           f"(the first ones, same mix), {cores} single-threaded "
-                                           "oracle workers"},
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
+        if rank == 0:
+            reference_main(args)
+        return  # the reference arm runs on rank 0's host cores alone
 
     import torch
 
@@ -409,326 +412,151 @@ def main():
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     else:
         torch.cuda.set_device(0)
     from ttnumpy_b200 import kernels as K
+    from ttnumpy_b200.persistent import prepare
 
     K.lib()
-    engine_kind = args.engine
-    eng = Engine(engine_kind)
-    dev_reqs = eng.upload(reqs)
-    flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB > L2
+    B = args.requests
+    n_value = (args.warmup + args.steps) * B
+    reqs = make_requests(n_value + args.serve_requests, args.seed, args.preset)
+    warm_reqs, timed_reqs = reqs[:args.warmup * B], reqs[args.warmup * B:n_value]
+    serve_reqs = reqs[n_value:]
+    kinds = [p.meta["kind"] for p in timed_reqs]
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        eng.solve_all(dev_reqs)
-    barrier()
-
-    lib = K.lib()
-    if engine_kind == "persistent":
-        return persistent_main(args, eng, dev_reqs, reqs, flush, barrier, world, rank, local)
-    # which kernel class dominates: one profiled pass, all classes
-    lib.ttb_profile_reset()
-    lib.ttb_profile_enable((1 << 12) - 1)
-    eng.solve_all(dev_reqs)
+    # inputs made resident before any timing
+    warm = prepare([(p.A, p.b, x0_host(p), solve_kwargs(p)) for p in warm_reqs])
+    timed = prepare([(p.A, p.b, x0_host(p), solve_kwargs(p)) for p in timed_reqs])
+    for p in warm + timed:
+        p.resident()
     torch.cuda.synchronize()
-    lib.ttb_profile_enable(0)
-    shares = profile_read(lib)
-    dominant = max(shares, key=lambda c: shares[c]["ms"])
-    lib.ttb_profile_reset()
-
-    # timed region: device time per step, L2 flushed between steps
-    step_ms, lats, ok, launches = [], [], 0, 0
+    if warm:
+        resident_run(args, warm, torch)
+    for p in warm:
+        p.drop_resident()
+    flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB > L2
+    K.fill_(flush, 0.0)
     barrier()
     with ClockSampler(local) as clocks:
-        lib.ttb_profile_enable(1 << dominant)
-        for _ in range(args.steps):
-            flush_l2(torch, flush)
-            torch.cuda.synchronize()
-            l0 = K.launch_count()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            results, lat = eng.solve_all(dev_reqs)
-            e.record()
-            torch.cuda.synchronize()
-            launches += K.launch_count() - l0
-            step_ms.append(s.elapsed_time(e))
-            lats.extend(lat)
-            ok += sum(1 for _, info in results if info.converged)
-        lib.ttb_profile_enable(0)
+        ms, jobs, launches, server = resident_run(args, timed, torch)
     barrier()
-    dom = profile_read(lib)[dominant]
-    value, total_ms = aggregate_rate(ok, sum(step_ms), world)
-
-    # end to end through the public API from pinned host buffers
-    e2e = e2e_run(eng, reqs, args, torch, flush)
-
-    if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
-        return
-    pk = peaks()
-    fp64 = fp64_peak_tflops(K, torch)
-    roof = roofline(dominant, dom, pk, fp64)
-    cpu = None
-    if world == 1:
-        sample = cpu_sample(reqs, n_sample)
-        dt, res = cpu_run(sample, cores)
-        conv = sum(1 for r in res if str(r[1]) == "converged")
-        cpu = {"value": conv / dt, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{len(sample)} of the {len(reqs)} requests (same mix), one pass, "
-                         f"{cores} single-threaded oracle workers"}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config(args, reqs, engine_kind),
-            "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
-            "converged": f"{ok}/{len(reqs) * args.steps}",
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(),
-            "kernel_shares": {CLASS_NAMES[c]: round(v["ms"], 3) for c, v in shares.items()
-                              if v["ms"] > 0}}
-    print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
-
-
-def persistent_main(args, eng, batch, reqs, flush, barrier, world, rank, local):
-    """Timed region for the persistent engine: one launch per step.  Steps
-    alternate between two device-resident copies of the batch on two
-    streams, so a step's last (longest-running) solves overlap the next
-    step's first ones, as back-to-back batches do in service; a copy is
-    launched again only after its previous step has been collected."""
-    import torch
-
-    from ttnumpy_b200 import kernels as K
-
-    batches = [batch, eng.upload(reqs)]
-    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
-    ok, lats, flops = 0, [], 0.0
-
-    def collect(j):
-        nonlocal ok, flops
-        with torch.cuda.stream(streams[j]):  # host reads on the batch's own stream
-            res = batches[j].collect()
-            lats.extend(batches[j].latencies_ms())
-            flops += batches[j].gemm_flops()
-        ok += sum(1 for r in res if r.status == 0 and r.info.converged)
-
-    barrier()
-    with ClockSampler(local) as clocks:
-        K.fill_(flush, 0.0)
-        torch.cuda.synchronize()
-        l0 = K.launch_count()
-        start = torch.cuda.Event(enable_timing=True)
-        start.record()
-        done = [None, None]
-        for k in range(args.steps):
-            j = k % 2
-            if done[j] is not None:
-                done[j].synchronize()
-                collect(j)
-            streams[j].wait_event(start)
-            batches[j].launch(streams[j])
-            done[j] = torch.cuda.Event()
-            done[j].record(streams[j])
-        for k in range(max(0, args.steps - 2), args.steps):
-            done[k % 2].synchronize()
-            collect(k % 2)
-        cur = torch.cuda.current_stream()
-        for st in streams:
-            cur.wait_stream(st)
-        end = torch.cuda.Event(enable_timing=True)
-        end.record()
-        torch.cuda.synchronize()
-        launches = K.launch_count() - l0
-    step_ms = [start.elapsed_time(end)]
-    barrier()
-    value, total_ms = aggregate_rate(ok, sum(step_ms), world)
-    for b in batches:  # the served run admits its own requests by device memory
-        b.release()
+    solved = [_solved(j) for j in jobs]
+    dev_s = [j.result.device_ms * 1e-3 if j.result is not None else 0.0 for j in jobs]
+    flops = sum(j.result.flops for j in jobs if j.result is not None)
+    peak_gb = server.peak_bytes / 2**30
+    value, total_ms = aggregate_rate(sum(solved), ms, world)
+    lats = [1e3 * j.latency for j in jobs if j.latency is not None]
+    jobs = server = None
+    for p in timed:
+        p.drop_resident()
+    del flush
     torch.cuda.empty_cache()
-    e2e = served_run(reqs, args, torch, rate=args.serve_rate or 2.0 * value / world)
-    e2e["value"], _ = aggregate_rate(e2e.pop("_solved"), 1e3 * e2e.pop("_seconds"), world)
-    plain = plain_run(reqs, args) if (world == 1 and args.plain_sample > 0) else None
+
+    # end to end through the server's public API from host memory
+    cap = value / world
+    sat = served_pass(args, serve_reqs, 2.0 * cap, torch, args.seed + 1)
+    loads = []
+    for f in [float(v) for v in args.serve_loads.split(",") if v.strip()]:
+        r = served_pass(args, serve_reqs, f * cap, torch, args.seed + 2)
+        loads.append({"load": f, "rate": r["rate"], "throughput": r["throughput"],
+                      "solved": f"{r['solved']}/{r['requests']}", "latency_ms": r["latency_ms"]})
+    e2e_value, _ = aggregate_rate(sat["solved"], 1e3 * sat["seconds"], world)
+    n_pass = max(1, sat["requests"])
+    e2e = {"value": e2e_value, "unit": UNIT,
+           "h2d_bytes_per_step": int(sat["h2d"] * B / n_pass),
+           "d2h_bytes_per_step": int(sat["d2h"] * B / n_pass),
+           "mode": f"served: {sat['requests']} requests of the stream from host memory arriving "
+                   f"as a Poisson stream at {sat['rate']:.2f}/s (twice the measured capacity), "
+                   f"continuous batching over {args.streams} streams of persistent launches of "
+                   f"at most {args.max_batch} requests admitted by a {args.serve_mem_gb:g} GB "
+                   "work-area budget, inputs copied per launch, solutions read back; bytes per "
+                   f"step scaled to {B} requests",
+           "solved": f"{sat['solved']}/{sat['requests']}",
+           "latency_ms": sat["latency_ms"], "peak_work_gb": sat["peak_gb"],
+           "launches": sat["launches"], "sustainable_load": loads}
+
+    plain = None
+    if world == 1 and args.plain_sample > 0:
+        plain = plain_run(reqs[:args.plain_sample], args.plain_limit, torch)
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
         return
     fp64 = fp64_peak_tflops(K, torch)
-    ach = flops / (sum(step_ms) * 1e-3) / 1e12
+    ach = flops / (ms * 1e-3) / 1e12
     roof = {"kernel": "k_amen (ttb_amen_persistent)", "bound": "tensor", "unit": "TFLOP/s",
             "achieved": ach, "peak": fp64, "peak_source": "measured FP64 FMA probe "
             "(ttb_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
-            "frac": ach / fp64, "traffic": _traffic(args),
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
-                              f"this workload (profiles/k_amen_bench_{args.requests}req.md)",
-            "flops_counted": "2mnk of every dense product the blocks ran; QR/SVD/LU not counted",
-            "per_launch_us": 1e3 * sum(step_ms) / args.steps, "launches": args.steps,
-            "timing": "aggregate over the timed steps (consecutive launches overlap on two "
-                      "streams)"}
+            "frac": ach / fp64, "traffic": None,
+            "traffic_source": "not measured for this workload in this run (ncu DRAM counters "
+                              "come from a separate small-case capture)",
+            "flops_counted": "2mnk of every dense product and 2 nnz n of every sparse "
+                             "operator-core product the blocks ran; QR/SVD/LU not counted",
+            "timing": "device time of the whole timed run (all steps' requests queued at once)"}
     cpu = None
     if world == 1:
-        n_sample = args.cpu_sample or min(len(reqs), max(2 * cpu_cores(), 8))
-        sample = cpu_sample(reqs, n_sample)
-        dt, res = cpu_run(sample, cpu_cores())
-        conv = sum(1 for r in res if str(r[1]) == "converged")
-        cpu = {"value": conv / dt, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
-               "sample": f"{len(sample)} of the {len(reqs)} requests (same mix), one pass, "
-                         f"{cpu_cores()} single-threaded oracle workers"}
+        n_cpu = args.cpu_sample or 2 * cpu_cores()
+        cpu = cpu_baseline(reqs[:n_cpu], cpu_cores(), args.cpu_limit)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config(args, reqs, "persistent"),
+            "data": "synthetic", "config": config(args),
+            "solved": f"{sum(solved)}/{len(solved)}",
+            "classes": class_stats(kinds, solved, dev_s),
             "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
-            "converged": f"{ok}/{len(reqs) * args.steps}", "roofline": roof,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "plain_gpu": plain,
-            "clocks": clocks.summary()}
+            "peak_work_gb": peak_gb,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "plain_gpu": plain, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-CLASS_NAMES = ["gemm", "copy", "kron", "norm", "local_matrix", "qr", "svd", "lu", "rank",
-               "minres", "gmres", "round"]
-
-
-def profile_read(lib):
-    import ctypes as C
-
-    out = {}
-    for c in range(len(CLASS_NAMES)):
-        ms, n, fl, by = C.c_double(), C.c_longlong(), C.c_double(), C.c_double()
-        lib.ttb_profile_read(c, C.byref(ms), C.byref(n), C.byref(fl), C.byref(by))
-        out[c] = {"ms": ms.value, "n": n.value, "flops": fl.value, "bytes": by.value}
-    return out
-
-
-def roofline(cls, rec, pk, fp64_tflops):
-    """Achieved algorithmic rate of the dominant kernel class over the
-    timed region against its measured peak."""
-    name = CLASS_NAMES[cls]
-    if rec["n"] == 0 or rec["ms"] <= 0:
-        return {"kernel": name, "bound": None, "achieved": None, "peak": None, "frac": None,
-                "traffic": None}
-    if rec["flops"] > 0:
-        ach = rec["flops"] / (rec["ms"] * 1e-3) / 1e12
-        return {"kernel": name, "bound": "tensor", "unit": "TFLOP/s", "achieved": ach,
-                "peak": fp64_tflops, "peak_source": "measured FP64 FMA probe (ttb_fma_peak)",
-                "frac": ach / fp64_tflops, "traffic": None,
-                "per_launch_us": 1e3 * rec["ms"] / rec["n"], "launches": rec["n"]}
-    gbs = rec["bytes"] / (rec["ms"] * 1e-3) / 1e9
-    peak = pk.get("hbm_gbs", 6650.0)
-    return {"kernel": name, "bound": "hbm", "unit": "GB/s", "achieved": gbs, "peak": peak,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
-            "frac": gbs / peak, "traffic": None, "per_launch_us": 1e3 * rec["ms"] / rec["n"],
-            "launches": rec["n"]}
-
-
-def served_run(reqs, args, torch, rate):
-    """End to end through the serving API: the requests (host cores) arrive
-    as a seeded Poisson stream at ``rate`` per second and are served by
-    continuous batching on concurrent persistent launches (inputs copied to
-    the device per launch, solutions read back).  ``args.steps`` passes,
-    each timed with CUDA events around the whole stream."""
-    from ttnumpy_b200.persistent_serving import PersistentServer
-
-    n_serve = args.serve_requests or 3 * len(reqs)
-    batch_host = [(p.A, p.b, Engine.x0_host(p), solve_kwargs(p)) for p in reqs]
-    host = [batch_host[i % len(batch_host)] for i in range(n_serve)]
-    rng = np.random.default_rng(args.seed + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(host)))
-    arrivals -= arrivals[0]
-    budget = int(args.serve_mem_gb * 2**30)
-    # untimed warm-up of the serving path (streams, pinned staging, allocator)
-    warm = min(len(host), 64)
-    PersistentServer(mem_budget=budget).serve(host[:warm], list(arrivals[:warm] * 0.0))
-    torch.cuda.synchronize()
-    seconds, solved, lats, launches, h2d, d2h, peak = 0.0, 0, [], 0, 0, 0, 0
-    steps = max(1, args.steps)
-    for _ in range(steps):
-        server = PersistentServer(mem_budget=budget)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        jobs = server.serve(host, list(arrivals))
-        torch.cuda.synchronize()
-        e.record()
-        e.synchronize()
-        seconds += s.elapsed_time(e) * 1e-3
-        solved += sum(1 for j in jobs if j.result.status == 0 and j.result.info.converged)
-        lats.extend(1e3 * j.latency for j in jobs)
-        launches += server.launches
-        h2d, d2h = server.h2d_bytes, server.d2h_bytes
-        peak = max(peak, server.peak_bytes)
-        # outside the timed region: drop this pass's results and return the
-        # cached blocks, so every pass starts from the same allocator state
-        jobs = server = None
-        torch.cuda.empty_cache()
-    return {"value": solved / seconds, "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h,
-            "mode": f"served: {len(host)} requests per step (the batch's {len(reqs)} cycled) "
-                    f"arriving as a Poisson stream at {rate:.1f}/s, continuous batching over 16 "
-                    f"streams of persistent launches admitted by a {args.serve_mem_gb:g} GB "
-                    "slab budget, inputs copied from host per launch, solutions read back",
-            "requests_per_step": len(host),
-            "peak_slab_gb": peak / 2**30,
-            "launches_per_step": launches / steps,
-            "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
-            "_seconds": seconds, "_solved": solved}
-
-
-def plain_run(reqs, args):
-    """The plain one-solve-at-a-time GPU AMEn (the drop-in ``amen``) on the
-    first requests of the mix, for the served-versus-plain ratio."""
-    import torch
-
-    eng = Engine("plain")
-    sample = reqs[: args.plain_sample]
-    handle = eng.upload(sample)
-    eng.solve_all(handle[:1])
-    torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    results, _ = eng.solve_all(handle)
-    e.record()
-    torch.cuda.synchronize()
-    ok = sum(1 for _, info in results if info.converged)
-    return {"value": ok / (s.elapsed_time(e) * 1e-3), "unit": UNIT,
-            "sample": f"the first {len(sample)} requests of the mix, solved one after another by "
-                      "the drop-in amen (every contraction and factorisation a library call)"}
-
-
-def e2e_run(eng, reqs, args, torch, flush):
-    """Same metric through the public API: each step uploads the requests
-    from host memory and downloads the solutions."""
-    from ttnumpy_b200 import kernels as K
-
-    total, ok, d2h, h2d = 0.0, 0, 0, 0
-    steps = max(1, args.steps)
-    for _ in range(steps):
-        K.fill_(flush, 0.0)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        handle = eng.upload(reqs)
-        results, _ = eng.solve_all(handle, download=False)
-        host = [x.to_numpy() for x, _ in results]
-        e.record()
-        torch.cuda.synchronize()
-        total += s.elapsed_time(e)
-        ok += sum(1 for _, info in results if info.converged)
-        d2h = sum(sum(c.nbytes for c in h) for h in host)
-        h2d = sum(sum(np.asarray(c).nbytes for c in p.A) + sum(np.asarray(c).nbytes for c in p.b)
-                  for p in reqs)
-    return {"value": ok / (total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h}
+def reference_main(args):
+    """The reference arm: the CPU oracle on the host cores.  Each step
+    solves the next ``cores`` requests of the stream (one per worker), each
+    capped at ``--cpu-limit`` seconds; warm-up steps solve one small
+    request per worker."""
+    cores = cpu_cores()
+    B = args.requests
+    reqs = make_requests((args.warmup + args.steps) * B, args.seed, args.preset)
+    small = [p for p in reqs if p.meta["kind"] == "qtt"][:cores] or reqs[:1]
+    for _ in range(args.warmup):
+        cpu_run(small, cores, args.cpu_limit)
+    total, cpu_s, res_all = 0.0, 0.0, []
+    for k in range(args.steps):
+        start = (args.warmup + k) * B
+        sample = reqs[start:start + min(cores, B)]
+        dt, res = cpu_run(sample, cores, args.cpu_limit)
+        total += dt
+        cpu_s += sum(r[0] for r in res)
+        res_all += res
+    solved = sum(1 for r in res_all if r[1])
+    value = solved / (cpu_s / cores)
+    sample_txt = (f"{min(cores, B)} requests per step (the first of each step's batch of the "
+                  "stream), "
+                  f"{cores} single-threaded oracle workers, each solve capped at "
+                  f"{args.cpu_limit:g} s; value = solved / (sum of solve seconds / cores)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(args, engine="reference"),
+            "solved": f"{solved}/{len(res_all)}",
+            "classes": class_stats([r[2] for r in res_all], [r[1] for r in res_all],
+                                   [r[0] for r in res_all]),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample_txt},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def percentile(v, q):
@@ -737,27 +565,23 @@ def percentile(v, q):
     return float(np.percentile(np.asarray(v, dtype=np.float64), q))
 
 
-def config(args, reqs, engine="reference"):
-    kinds = {}
-    for p in reqs:
-        kinds[p.meta["kind"]] = kinds.get(p.meta["kind"], 0) + 1
-    return {"workload": "AMEn request mix: 2-D QTT Poisson (6-20 cores, mode 2) and parametric "
-                        f"diffusion (d in {args.diffusion_dims}, mode in {args.diffusion_modes}), "
-                        "residual 1e-8",
-            "requests_per_step": len(reqs), "mix": kinds, "engine": engine,
-            "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
-            "parallelism": f"replicas x{args.gpus}", **_timing_notes(engine)}
-
-
-def _timing_notes(engine):
-    if engine == "persistent":
-        return {"l2": "inputs larger than L2 (two batches of slabs, tens of GB); 512 MB flush "
-                      "before the timed region",
-                "steps": "alternate between two device-resident copies of the batch on two "
-                         "streams, so one step's last solves overlap the next step's first"}
-    if engine == "reference":
-        return {"host": "the CPU oracle on the host cores; no device memory involved"}
-    return {"l2": "flushed (512 MB write) before every timed step"}
+def config(args, engine="persistent server"):
+    if args.preset == "config5":
+        work = ("AMEn serving mix (stream of requests): 10% large diffusion d=24 n=64 with "
+                "rank-8 right-hand side, 45% parametric diffusion d~U{4..12} n~U{16,32,64}, 45% "
+                "2-D QTT Poisson with 6-20 cores; residual 1e-8, at most 30 sweeps")
+    else:
+        work = ("AMEn reduced mix: 2-D QTT Poisson (6-20 cores) and parametric diffusion "
+                "(d in 4,5, n in 16,32); residual 1e-8, at most 30 sweeps")
+    out = {"workload": work, "requests_per_step": args.requests, "engine": engine,
+           "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
+           "parallelism": f"replicas x{args.gpus}"}
+    if engine != "reference":
+        out["l2"] = ("inputs larger than L2 (each request's work area is tens to hundreds of "
+                     "MB); 512 MB flush before the timed region")
+        out["steps"] = ("the timed steps' requests (consecutive batches of the stream) queued "
+                        "at once, longest first, to the server on device-resident inputs")
+    return out
 
 
 if __name__ == "__main__":

@@ -448,7 +448,8 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * ``slab`` (ttb_amen_slab_doubles() doubles); x bonds are capped at
  * ``rmax`` (status -4 when a bond would exceed it).  Results: result[0]
  * status (0 ok, -1 singular local system, -3 slab too small, -4 rank cap,
- * -5 unsupported settings, -6 time limit), result[1] sweeps run,
+ * -5 unsupported settings, -6 time limit, -7 tensor-core pipeline),
+ * result[1] sweeps run,
  * result[2] stop reason (0 converged, 1 stagnated, 2 max sweeps),
  * result[3] local solves,
  * result[4] inexact local solves, result[5..5+d] x bonds;
@@ -461,7 +462,7 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * products (a part of the other phases), residual checks and set-up,
  * residuals[2 * max_sweeps + 10] and [+ 11] the device's global timer (ns)
  * when the block started and finished the solve (``residuals`` holds
- * 2 * max_sweeps + 14 doubles); x core k at
+ * 2 * max_sweeps + 16 doubles); x core k at
  * slab + x_offsets[k].  Blocks start in task order, so listing the longest
  * solves first shortens the launch.  local_rtol > 0
  * selects MINRES for local systems above direct_solve_size unknowns (at
@@ -498,6 +499,13 @@ typedef struct {
                               per-solve time limit of the reference's
                               benchmark runner, benchmarks/poisson.py:95-143);
                               sweeps, residuals and bonds so far are kept */
+  int precision;           /* 0: float64 throughout; 1: mixed: iterative local
+                              solves by float64 iterative refinement around
+                              inner MINRES solves whose operator products run
+                              on the tensor cores in 3xTF32 (residuals
+                              [2*max_sweeps + 14] receives their FLOPs, [+ 15]
+                              the refinement steps; status -7 if a tensor-core
+                              wait gave up) */
 } ttb_amen_task_t;
 long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int rmax,
                                 int direct_solve_size);

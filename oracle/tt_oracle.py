@@ -459,6 +459,21 @@ def tt_norm(t: Train) -> float:
     return float(np.linalg.norm(cores[0].reshape(-1)))
 
 
+def inner(a, b) -> float:
+    """Inner product <a, b> of two TT vectors given as core lists (or
+    Trains) of equal mode sizes, by a left-to-right contraction of the
+    cores: a fingerprint of a solution that does not depend on its gauge
+    (QR/SVD signs), used to compare solutions without storing their cores."""
+    ca = a.cores if hasattr(a, "cores") else a
+    cb = b.cores if hasattr(b, "cores") else b
+    env = np.ones((1, 1))
+    for x, y in zip(ca, cb):
+        x = np.asarray(x).reshape(x.shape[0], -1, x.shape[-1])
+        y = np.asarray(y).reshape(y.shape[0], -1, y.shape[-1])
+        env = np.einsum("ab,anc,bnd->cd", env, x, y)
+    return float(env[0, 0])
+
+
 def relative_residual(A: Train, b: Train, x: Train, b_norm: Optional[float] = None) -> float:
     """``||A x - b|| / ||b||`` in TT arithmetic (``solvers/common.py:118-146``)."""
     res = add(dot(A, x), scale(b, -1.0))
@@ -809,12 +824,23 @@ def amen(A: Train, b: Train, x0: Optional[Train] = None, kickrank=4, error_thres
          max_rank=None, max_sweeps=1, residual_tol=None, residual_damp=2.0,
          stagnation_factor="auto", local_solver="auto", direct_solve_size=1000,
          local_rtol=None, allow_dense_fallback=False, symmetric=False, seed=None,
-         return_info=True):
+         return_info=True, time_limit=None):
     """AMEn one-site sweep with residual enrichment (``solvers/amen.py:395-725``).
 
     Returns ``(x, info)``.  The per-sweep monitor restates
-    ``_SweepMonitor.record`` (``solvers/common.py:504-592``).
+    ``_SweepMonitor.record`` (``solvers/common.py:504-592``).  With
+    ``time_limit`` (seconds, host clock) the solve stops after the first
+    local step that ends past it, with stop reason "time_limit" (the
+    per-solve limit of the reference's benchmark runner,
+    ``benchmarks/poisson.py:95-143``); the solution is then not valid.
     """
+    import time as _time
+
+    t_start = _time.perf_counter()
+
+    def over_time():
+        return time_limit is not None and _time.perf_counter() - t_start > time_limit
+
     if kickrank <= 0:
         raise ValueError("kickrank must be a positive integer")
     if max_rank is not None and max_rank <= 0:
@@ -866,6 +892,9 @@ def amen(A: Train, b: Train, x0: Optional[Train] = None, kickrank=4, error_thres
             block = np.einsum("ba,bin->ain", E["lxz"][k], z_new)
             enrich_right(x, k, core, carry, block, max_rank)
             shift_right(z, k, z_new)
+            if over_time():
+                info.stop_reason = "time_limit"
+                return x, info
         build_left(d - 1)
         for k in range(d - 1, -1, -1):
             build_right(k)
@@ -882,6 +911,9 @@ def amen(A: Train, b: Train, x0: Optional[Train] = None, kickrank=4, error_thres
                 block = _mul_right(z_new, E["rxz"][k])
                 enrich_left(x, k, core, carry, block, max_rank)
                 shift_left(z, k, z_new)
+            if over_time():
+                info.stop_reason = "time_limit"
+                return x, info
         info.num_sweeps_run = sweep + 1
         info.max_bonds.append(max(x.bonds))
         if st.track_residual:

@@ -10,6 +10,7 @@ reference checkout (the directory holding the ``ttnumpy`` package)::
     python tests/golden/make_golden.py hadamard # element-wise products only
     python tests/golden/make_golden.py canonical  # canonical_tt only
     python tests/golden/make_golden.py tt_svd   # TT-SVD only
+    python tests/golden/make_golden.py serving  # the serving mix's classes only
     python tests/golden/make_golden.py tt_to_qtt  # quantisation only
 
 Each case is written to ``tests/golden/<name>.npz`` with its inputs (train
@@ -306,7 +307,57 @@ def tt_to_qtt_cases() -> None:
     save("tt_to_qtt", data, {"cases": cases, "back": back})
 
 
+#: seeds of the probe trains whose inner products with a solution are
+#: stored as its fingerprint (rank-2 uniform trains, ``P.random_tt``)
+PROBE_SEEDS = (101, 102, 103)
+
+
+def serving_cases() -> None:
+    """AMEn on the request classes of the serving mix at their full sizes:
+    parametric diffusion with d up to 12 and mode size 64, and the large
+    class (d = 24, n = 64, rank-8 right-hand side).  Their cores are
+    regenerated by the tests from the stored draw (problems.py), and the
+    solution is stored as a fingerprint (norm, inner products with seeded
+    probe trains) instead of its cores; the shorter runs are prefixes of
+    the trajectory (max_sweeps below convergence)."""
+    sys.path.insert(0, ROOT)
+    from oracle.tt_oracle import inner
+
+    kw = dict(residual_tol=1e-8, symmetric=True, seed=0, stagnation_factor=None)
+    cases = [("amen_c5_diffusion_d4_n64", "diffusion", 4, 64, 21, 30),
+             ("amen_c5_diffusion_d8_n64", "diffusion", 8, 64, 22, 4),
+             ("amen_c5_diffusion_d12_n32", "diffusion", 12, 32, 23, 4),
+             ("amen_c5_large", "large", 24, 64, 24, 6)]
+    for name, kind, d, n, seed, sweeps in cases:
+        g = np.random.default_rng(seed)
+        theta = g.uniform(-1.0, 1.0, size=d)
+        rhs_seed = int(g.integers(1 << 31))
+        p = (P.parametric_diffusion(d, n, theta) if kind == "diffusion"
+             else P.large_diffusion(theta, rhs_seed, n))
+        A, b = ref_train(p.A), ref_train(p.b)
+        t0 = time.perf_counter()
+        x, info = tt.amen(A, b, return_info=True, max_sweeps=sweeps, **kw)
+        elapsed = time.perf_counter() - t0
+        data = {"theta": theta, "rhs_seed": np.array(rhs_seed),
+                "residuals": np.array(info.residuals, dtype=np.float64),
+                "max_bonds": np.array(info.max_bonds), "bonds": np.array(x.bonds),
+                "num_sweeps_run": np.array(info.num_sweeps_run),
+                "stop_reason": np.array(str(info.stop_reason)),
+                "local_solves": np.array(info.local_solves),
+                "local_inexact": np.array(info.local_inexact),
+                "final_residual": np.array(relative_residual(A, b, x)),
+                "x_norm": np.array(x.tt_norm()),
+                "probe_seeds": np.array(PROBE_SEEDS),
+                "probes": np.array([inner(x.cores, P.random_tt([n] * d, 2, seed=s))
+                                    for s in PROBE_SEEDS]),
+                "seconds": np.array(elapsed)}
+        save(name, data, dict(kw, max_sweeps=sweeps, kind=kind, d=d, n=n))
+
+
 def main() -> None:
+    if "serving" in sys.argv[1:]:
+        serving_cases()
+        return
     if "tt_to_qtt" in sys.argv[1:]:
         tt_to_qtt_cases()
         return
@@ -448,6 +499,7 @@ def main() -> None:
     canonical_cases()
     tt_svd_cases()
     tt_to_qtt_cases()
+    serving_cases()
 
     with open(os.path.join(HERE, "meta.json"), "w") as fh:
         json.dump(meta, fh, indent=1)

@@ -11,8 +11,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_reference_arm_json_line():
     cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-           "--requests", "4", "--cpu-sample", "2", "--steps", "1", "--warmup", "0",
-           "--diffusion-dims", "4", "--diffusion-modes", "16"]
+           "--preset", "small", "--requests", "4", "--steps", "1", "--warmup", "0",
+           "--cpu-limit", "10"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True).stdout
     lines = [ln for ln in out.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
@@ -27,6 +27,8 @@ def test_reference_arm_json_line():
     assert set(d["e2e"]) >= {"value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"}
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["config"]["workload"] and d["config"]["requests_per_step"] == 4
+    # per-class counts of the sampled requests
+    assert sum(c["requests"] for c in d["classes"].values()) == 4
 
 
 def test_reference_arm_other_ranks_exit_quietly():

@@ -15,6 +15,7 @@
 
 #include "ttb200.h"
 #include "ttb_device.cuh"
+#include "ttb_tc_block.cuh"
 
 namespace ttb {
 void count_launch();  // the library's launch counter (ttb200.cu)
@@ -39,7 +40,8 @@ constexpr double kShrink = 1e-2;       // common.py:233
 constexpr int kMaxMinres = 2000;       // iteration cap of one MINRES call
 constexpr double kEps = 2.220446049250313e-16;
 
-enum { ST_OK = 0, ST_SINGULAR = -1, ST_SLAB = -3, ST_RANK = -4, ST_SETTINGS = -5, ST_TIME = -6 };
+enum { ST_OK = 0, ST_SINGULAR = -1, ST_SLAB = -3, ST_RANK = -4, ST_SETTINGS = -5, ST_TIME = -6,
+       ST_TENSOR = -7 };
 enum { F_A = 0, F_B, F_ZB, F_ZAX, F_XZ };
 
 struct Sm {
@@ -51,6 +53,8 @@ struct Sm {
   int ipiv[LNB];
   int flag;
   i64 stack0;
+  uint64_t mbar[TC_STAGES];  // tensor-core pipeline (mixed precision)
+  uint32_t tmem_slot;
 };
 
 struct Ctx {
@@ -69,6 +73,10 @@ struct Ctx {
   double check_qr;        // debug: worst relative gap of the two-level R-only QR
   int n_qr2;              // debug: two-level R-only QRs checked
   long long cyc[8];       // SM cycles per phase (see PH_*)
+  int mixed;              // 3xTF32 inner solves with float64 refinement
+  TcState tc;             // the block's tensor-core pipeline (mixed only)
+  double flops_tc;        // FLOPs of the tensor-core products
+  long long refine;       // float64 refinement steps of the local solves
 };
 
 // the device-wide nanosecond timer (comparable across SMs)
@@ -130,6 +138,140 @@ __device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, OMat C, int M, int N, 
   c.cyc[PH_GEMM] += clock64() - t0;
 }
 
+// The product on the tensor cores in 3xTF32 (``tc``) or in float64.
+__device__ __forceinline__ void gemm_any(Ctx& c, bool tc, CMat A, CMat B, OMat C, int M, int N,
+                                         int K, double alpha, double beta) {
+  if (!tc || K <= 0) {
+    gemm(c, A, B, C, M, N, K, alpha, beta);
+    return;
+  }
+  if (M <= 0 || N <= 0) return;
+  c.flops_tc += 2.0 * M * N * (double)K;
+  const long long t0 = clock64();
+  cta_gemm_tc(c.tc, A, B, C, M, N, K, alpha, beta);
+  if (c.tc.failed) c.status = ST_TENSOR;
+  c.cyc[PH_GEMM] += clock64() - t0;
+}
+
+// ---------------------------------------------------------------------------
+// operator cores as sparse matrices
+// ---------------------------------------------------------------------------
+
+// A TTM core op (R, n, m, R2) viewed as a matrix over two of its index pairs
+// and stored by rows in compressed form with its exact zeros dropped.  The
+// cores of discretised operators are block-banded (identity, diagonal and
+// tridiagonal n x m blocks, most (a, b) blocks zero), so a product with the
+// core touches a few percent of the dense core's entries; the result is the
+// dense product's up to the order in which the nonzero terms are summed.
+//   SP_X: rows (k, b), columns (a, l) (the one-site operator's middle product)
+//   SP_T: rows (l, b), columns (a, k) (left environment updates)
+//   SP_P: rows (a, k), columns (l, b) (the core's own row-major layout)
+enum { SP_X = 0, SP_T = 1, SP_P = 2 };
+struct SpOp {
+  const int* ptr;  // rows + 1 row starts
+  const int* col;
+  const double* val;
+  int rows;  // 0: no sparse form (the dense product is used)
+  int nnz;
+};
+
+// Cores below this many entries, or denser than one nonzero in kSpDensity,
+// keep the dense product.
+constexpr int kSpMinEntries = 4096;
+constexpr int kSpDensity = 4;
+
+// Stack doubles a sparse form of an R * n * m * R2 core may take.
+__host__ __device__ constexpr i64 spop_doubles(i64 entries, i64 rows) {
+  return (rows + 2) / 2 + 1 + 3 * (entries / kSpDensity + 1) / 2 + 96;
+}
+
+__device__ __forceinline__ i64 sp_index(int pairing, int row, int col, int R, int n, int m,
+                                        int R2) {
+  int a, k, l, b;
+  if (pairing == SP_X) {
+    k = row / R2, b = row % R2, a = col / m, l = col % m;
+  } else if (pairing == SP_T) {
+    l = row / R2, b = row % R2, a = col / n, k = col % n;
+  } else {
+    return (i64)row * m * R2 + col;
+  }
+  return (((i64)a * n + k) * m + l) * R2 + b;
+}
+
+// Builds the sparse form of ``op`` on the stack (left there for the caller's
+// mark to release).  S.rows == 0 when the core is small or dense.
+__device__ __noinline__ SpOp build_spop(Ctx& c, const double* op, int R, int n, int m, int R2,
+                                        int pairing) {
+  SpOp S{nullptr, nullptr, nullptr, 0, 0};
+  const i64 entries = (i64)R * n * m * R2;
+  if (entries < kSpMinEntries) return S;
+  const int rows = pairing == SP_X ? n * R2 : pairing == SP_T ? m * R2 : R * n;
+  const int cols = (int)(entries / rows);
+  const i64 cap = entries / kSpDensity + 1;
+  int* ptr = reinterpret_cast<int*>(take(c, (rows + 2) / 2 + 1));
+  double* val = take(c, cap);
+  int* col = reinterpret_cast<int*>(take(c, (cap + 1) / 2));
+  if (c.status) return S;
+  for (int r = threadIdx.x; r < rows; r += TTB_THREADS) {
+    int cnt = 0;
+    for (int q = 0; q < cols; ++q) cnt += (op[sp_index(pairing, r, q, R, n, m, R2)] != 0.0);
+    ptr[r + 1] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ptr[0] = 0;
+    for (int r = 0; r < rows; ++r) ptr[r + 1] += ptr[r];
+  }
+  __syncthreads();
+  const int nnz = ptr[rows];
+  if ((i64)nnz > cap - 1) return S;  // too dense: dense product
+  for (int r = threadIdx.x; r < rows; r += TTB_THREADS) {
+    int e = ptr[r];
+    for (int q = 0; q < cols; ++q) {
+      const double v = op[sp_index(pairing, r, q, R, n, m, R2)];
+      if (v != 0.0) {
+        val[e] = v;
+        col[e] = q;
+        ++e;
+      }
+    }
+  }
+  __syncthreads();
+  S.ptr = ptr;
+  S.col = col;
+  S.val = val;
+  S.rows = rows;
+  S.nnz = nnz;
+  return S;
+}
+
+// C[r, j] = alpha * sum_e val[e] B[col[e], j] + beta * C[r, j] for r < S.rows,
+// j < N, with B[q, j] = B[q * b_rs + j * b_cs] and C addressed through an
+// OMat.  Warps take rows, lanes take columns; each element sums its row's
+// nonzero terms in column order, so the result does not depend on the
+// schedule.  beta == 0 never reads C.
+__device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_rs, i64 b_cs,
+                                  OMat C, int N, double alpha, double beta) {
+  c.flops += 2.0 * S.nnz * (double)N;
+  const long long t0 = clock64();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r = warp; r < S.rows; r += TTB_WARPS) {
+    const int e0 = S.ptr[r], e1 = S.ptr[r + 1];
+    double* crow = C.p + C.row(r);
+    for (int j = lane; j < N; j += 32) {
+      const double* bj = B + (i64)j * b_cs;
+      double acc = 0.0;
+      for (int e = e0; e < e1; ++e) acc = fma(S.val[e], bj[(i64)S.col[e] * b_rs], acc);
+      double* cp = crow + C.col(j);
+      double v = alpha * acc;
+      if (beta != 0.0) v = fma(beta, *cp, v);
+      *cp = v;
+    }
+  }
+  __syncthreads();
+  c.cyc[PH_GEMM] += clock64() - t0;
+}
+
 // ---------------------------------------------------------------------------
 // environments (common.py:149-217), same GEMM chains as ttb_env_update
 // ---------------------------------------------------------------------------
@@ -147,8 +289,14 @@ __device__ __noinline__ void env_step(Ctx& c, int side, const double* env, int t
       gemm(c, CMat{env, f, 1}, CMat{frame, (i64)n * f2, 1},
            OMat(S1, R, f2, (i64)n * t * f2, f2, (i64)t * f2, 1), t * R, n * f2, f, 1.0, 0.0);
       // S2[i, l, b, q] = sum_{a, k} op[a, k, l, b] S1[(a, k), (i, q)]
-      gemm(c, CMat{op, 1, (i64)m * R2}, CMat{S1, (i64)t * f2, 1},
-           OMat(S2, kNoSplit, 0, f2, f2, (i64)m * R2 * f2, 1), m * R2, t * f2, R * n, 1.0, 0.0);
+      const SpOp S = build_spop(c, op, R, n, m, R2, SP_T);
+      if (c.status) return;
+      const OMat o2(S2, kNoSplit, 0, f2, f2, (i64)m * R2 * f2, 1);
+      if (S.rows)
+        spmm(c, S, S1, (i64)t * f2, 1, o2, t * f2, 1.0, 0.0);
+      else
+        gemm(c, CMat{op, 1, (i64)m * R2}, CMat{S1, (i64)t * f2, 1}, o2, m * R2, t * f2, R * n,
+             1.0, 0.0);
       gemm(c, CMat{target, 1, t2}, CMat{S2, (i64)R2 * f2, 1}, Mat{out, (i64)R2 * f2, 1}, t2,
            R2 * f2, t * m, 1.0, 0.0);
     } else {
@@ -159,8 +307,14 @@ __device__ __noinline__ void env_step(Ctx& c, int side, const double* env, int t
       gemm(c, CMat{target, t, 1}, CMat{env, (i64)R * f, 1},
            OMat(S1, m, f, (i64)R * t2 * f, f, (i64)t2 * f, 1), t2 * m, R * f, t, 1.0, 0.0);
       // S2[j, b, k, p] = sum_{l, a} op[b, k, l, a] S1[(l, a), (j, p)]
-      gemm(c, CMat{op, (i64)m * R, 1}, CMat{S1, (i64)t2 * f, 1},
-           OMat(S2, kNoSplit, 0, f, f, (i64)R2 * n * f, 1), R2 * n, t2 * f, m * R, 1.0, 0.0);
+      const SpOp S = build_spop(c, op, R2, n, m, R, SP_P);
+      if (c.status) return;
+      const OMat o2(S2, kNoSplit, 0, f, f, (i64)R2 * n * f, 1);
+      if (S.rows)
+        spmm(c, S, S1, (i64)t2 * f, 1, o2, t2 * f, 1.0, 0.0);
+      else
+        gemm(c, CMat{op, (i64)m * R, 1}, CMat{S1, (i64)t2 * f, 1}, o2, R2 * n, t2 * f, m * R,
+             1.0, 0.0);
       gemm(c, CMat{S2, (i64)n * f, 1}, CMat{frame, 1, (i64)n * f}, Mat{out, f2, 1}, t2 * R2, f2,
            n * f, 1.0, 0.0);
     }
@@ -243,6 +397,7 @@ struct LocalOp {
   const double* right;
   const double* opP;     // op re-laid out as [a, l, k, b] (permute_op)
   const double* rightP;  // right re-laid out as [b, p, q] (permute_op)
+  SpOp sx, sp;           // op's sparse forms SP_X and SP_P (permute_op), if any
   int lt, lf, R, R2, n, m, rt, rf;
 };
 
@@ -258,6 +413,7 @@ __device__ LocalOp local_A(Ctx& c, int k) {
   L.R2 = s->R[k + 1];
   L.n = L.m = s->n[k];
   L.opP = L.rightP = nullptr;
+  L.sx.rows = L.sp.rows = 0;
   return L;
 }
 
@@ -287,6 +443,9 @@ __device__ __noinline__ void permute_op(Ctx& c, LocalOp& L) {
   __syncthreads();
   L.opP = opP;
   L.rightP = rightP;
+  L.sx = build_spop(c, L.op, R, n, m, R2, SP_X);
+  if (c.status) return;
+  L.sp = L.sx.rows ? build_spop(c, L.op, R, n, m, R2, SP_P) : SpOp{nullptr, nullptr, nullptr, 0, 0};
 }
 
 // y = alpha * B x + beta * y for ``cols`` vectors (one_site.py:78-115) as
@@ -295,7 +454,7 @@ __device__ __noinline__ void permute_op(Ctx& c, LocalOp& L) {
 // permuted (split-index outputs) so that each next product reads plain
 // strides.  Needs permute_op(L).
 __device__ __noinline__ void apply(Ctx& c, const LocalOp& L, const double* x, double* y, int cols,
-                      double alpha, double beta) {
+                      double alpha, double beta, bool tc = false) {
   const int lt = L.lt, lf = L.lf, R = L.R, R2 = L.R2, n = L.n, m = L.m, rt = L.rt, rf = L.rf;
   const i64 mark = c.top;
   c.applies += cols;
@@ -306,14 +465,20 @@ __device__ __noinline__ void apply(Ctx& c, const LocalOp& L, const double* x, do
     const double* xc = x + (i64)cc * lt * m * rt;
     double* yc = y + (i64)cc * lf * n * rf;
     // W1[(a, j), (l, p)] = sum_i left[i, a, j] x[i, l, p]
-    gemm(c, CMat{L.left, 1, (i64)R * lf}, CMat{xc, (i64)m * rt, 1},
-         OMat(W1, lf, (i64)m * lf * rt, rt, rt, (i64)lf * rt, 1), R * lf, m * rt, lt, 1.0, 0.0);
+    gemm_any(c, tc, CMat{L.left, 1, (i64)R * lf}, CMat{xc, (i64)m * rt, 1},
+             OMat(W1, lf, (i64)m * lf * rt, rt, rt, (i64)lf * rt, 1), R * lf, m * rt, lt, 1.0,
+             0.0);
     // W2[(k, b), (j, p)] = sum_{a, l} op[a, k, l, b] W1[(a, l), (j, p)]
-    gemm(c, CMat{L.opP, 1, (i64)n * R2}, CMat{W1, (i64)lf * rt, 1},
-         OMat(W2, kNoSplit, 0, rt, rt, (i64)n * R2 * rt, 1), n * R2, lf * rt, R * m, 1.0, 0.0);
+    const OMat o2(W2, kNoSplit, 0, rt, rt, (i64)n * R2 * rt, 1);
+    if (L.sx.rows)
+      spmm(c, L.sx, W1, (i64)lf * rt, 1, o2, lf * rt, 1.0, 0.0);
+    else
+      gemm_any(c, tc, CMat{L.opP, 1, (i64)n * R2}, CMat{W1, (i64)lf * rt, 1}, o2, n * R2,
+               lf * rt, R * m, 1.0, 0.0);
     // y[(j, k), q] = alpha * sum_{b, p} W2[(j, k), (b, p)] right[p, b, q] + beta * y
-    gemm(c, CMat{W2, (i64)R2 * rt, 1}, CMat{L.rightP, rf, 1}, Mat{yc, rf, 1}, lf * n, rf,
-         R2 * rt, alpha, beta);
+    gemm_any(c, tc, CMat{W2, (i64)R2 * rt, 1}, CMat{L.rightP, rf, 1}, Mat{yc, rf, 1}, lf * n, rf,
+             R2 * rt, alpha, beta);
+    if (c.status) break;
   }
   c.top = mark;
 }
@@ -482,7 +647,7 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
 // MINRES, SciPy 1.18.1's algorithm and stopping rules (Paige & Saunders);
 // x holds the initial guess (warm) on entry and the iterate on exit.
 __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, double* x, i64 N, double rtol,
-                       int maxit, bool warm) {
+                       int maxit, bool warm, bool tc = false) {
   double* red = c.sm->red;
   const i64 mark = c.top;
   double* buf = take(c, 6 * N);
@@ -497,7 +662,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   double* w = buf + 4 * N;
   double* w2 = buf + 5 * N;
   if (warm) {
-    apply(c, L, x, y, 1, 1.0, 0.0);
+    apply(c, L, x, y, 1, 1.0, 0.0, tc);
     for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) r1[i] = b[i] - y[i];
   } else {
     vfill(x, N, 0.0);
@@ -525,7 +690,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     const double s = 1.0 / beta;
     for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) v[i] = s * r2[i];
     __syncthreads();
-    apply(c, L, v, y, 1, 1.0, 0.0);
+    apply(c, L, v, y, 1, 1.0, 0.0, tc);
     if (c.status) return;
     // y -= (beta / oldb) r1 and alfa = v . y in one pass
     double dot = 0.0;
@@ -609,6 +774,55 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   c.top = mark;
 }
 
+// Mixed-precision iterative local solve: float64 iterative refinement
+// around inner MINRES solves whose operator applications run on the tensor
+// cores in 3xTF32.  u holds the warm start on entry.  Each step computes the
+// residual r = b - B u with the float64 operator, solves B d = r with the
+// 3xTF32 operator to kInnerRtol, and adds d to u; the solve ends once
+// ||r|| <= local_rtol ||b|| (the reference's true-residual test,
+// common.py:776-809) or after kMaxRefine steps (then counted inexact, as the
+// reference counts a local solve that missed local_rtol).
+constexpr int kMaxRefine = 10;
+constexpr double kInnerRtol = 1e-5;
+
+__device__ __noinline__ void solve_refined(Ctx& c, const LocalOp& L, const double* b_loc,
+                                           double* u, i64 N, int maxit, int* nsolves,
+                                           int* ninexact) {
+  const ttb_amen_task_t* T = c.T;
+  double* red = c.sm->red;
+  const i64 mark = c.top;
+  double* r = take(c, N);
+  double* dlt = take(c, N);
+  if (c.status) return;
+  const double bn = vnorm_diff(b_loc, nullptr, N, red);
+  bool done = false;
+  for (int it = 0; it <= kMaxRefine; ++it) {
+    // r = b - B u in float64
+    apply(c, L, u, r, 1, -1.0, 0.0);
+    if (c.status) return;
+    double part = 0.0;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) {
+      const double v = r[i] + b_loc[i];
+      r[i] = v;
+      part = fma(v, v, part);
+    }
+    const double rn = sqrt(block_sum(part, red));
+    if (rn <= T->local_rtol * bn) {
+      done = true;
+      break;
+    }
+    if (it == kMaxRefine) break;
+    c.refine += 1;
+    minres(c, L, r, dlt, N, kInnerRtol, maxit, false, true);
+    if (c.status) return;
+    for (i64 i = threadIdx.x; i < N; i += TTB_THREADS) u[i] += dlt[i];
+    __syncthreads();
+  }
+  *nsolves += 1;
+  if (!done) *ninexact += 1;
+  c.top = mark;
+}
+
 // _solve_local_system (common.py:729-809): u <- solution of B u = b.
 __device__ __noinline__ void solve_local(Ctx& c, int k, const double* b_loc, double* u, int* nsolves,
                             int* ninexact) {
@@ -634,6 +848,11 @@ __device__ __noinline__ void solve_local(Ctx& c, int k, const double* b_loc, dou
   // SciPy's default cap is 5 N iterations; a block solving alone on one SM
   // is bounded tighter so that no launch runs unbounded on a shared GPU
   const int maxit = (int)min(5 * N, (i64)kMaxMinres);
+  if (c.mixed) {
+    solve_refined(c, L, b_loc, u, N, maxit, nsolves, ninexact);
+    if (!c.status) c.top = mark;
+    return;
+  }
   for (int attempt = 0; attempt < kMaxRestarts; ++attempt) {
     minres(c, L, b_loc, u, N, rtol, maxit, true);
     if (c.status) return;
@@ -724,15 +943,21 @@ __device__ __noinline__ void rank_chunk(Ctx& c, const LocalOp& L, bool forward, 
     gemm(c, CMat{L.left, 1, (i64)R * lf}, CMat{Up + (i64)c0 * m, (i64)p * m, 1},
          OMat(Y, lf, m, (i64)R * m, m, (i64)lf * R * m, 1), R * lf, nc * m, lt, 1.0, 0.0);
     // out[(r, j), (k, b)] = PP2[(r, j), (a, l)] opP[(a, l), (k, b)]
-    gemm(c, CMat{Y, (i64)R * m, 1}, CMat{L.opP, (i64)n * R2, 1}, Mat{out, (i64)n * R2, 1},
-         nc * lf, n * R2, R * m, 1.0, 0.0);
+    if (L.sx.rows)  // as out^T = op_X PP2^T
+      spmm(c, L.sx, Y, 1, (i64)R * m, OMat(Mat{out, 1, (i64)n * R2}), nc * lf, 1.0, 0.0);
+    else
+      gemm(c, CMat{Y, (i64)R * m, 1}, CMat{L.opP, (i64)n * R2, 1}, Mat{out, (i64)n * R2, 1},
+           nc * lf, n * R2, R * m, 1.0, 0.0);
   } else {
     // Y (Qt[(l, b)][(r, q)]) = Vh[c0:c0+nc, (l, p')] right[p', (b, q)], written permuted
     gemm(c, CMat{Vh + (i64)c0 * m * rt, rt, 1}, CMat{L.right, (i64)R2 * rf, 1},
          OMat(Y, m, rf, (i64)R2 * nc * rf, rf, (i64)nc * rf, 1), nc * m, R2 * rf, rt, 1.0, 0.0);
     // out[(a, k), (r, q)] = op[(a, k), (l, b)] Qt[(l, b), (r, q)]
-    gemm(c, CMat{L.op, (i64)m * R2, 1}, CMat{Y, (i64)nc * rf, 1}, Mat{out, (i64)nc * rf, 1},
-         R * n, nc * rf, m * R2, 1.0, 0.0);
+    if (L.sp.rows)
+      spmm(c, L.sp, Y, (i64)nc * rf, 1, OMat(Mat{out, (i64)nc * rf, 1}), nc * rf, 1.0, 0.0);
+    else
+      gemm(c, CMat{L.op, (i64)m * R2, 1}, CMat{Y, (i64)nc * rf, 1}, Mat{out, (i64)nc * rf, 1},
+           R * n, nc * rf, m * R2, 1.0, 0.0);
   }
 }
 
@@ -1229,9 +1454,16 @@ __device__ __noinline__ double train_norm(Ctx& c, int which) {
              OMat(T + (i64)bb * x1 * cp, n, cp, (i64)R2 * x1 * cp, kNoSplit, 0, 1), x1 * n, cp,
              x2, 1.0, 0.0);
       // mm[(a, xr), j, q] = sum_{l, b} A[a, j, l, b] T[(l, b), (xr, q)]
-      gemm(c, CMat{acore(c, i), (i64)n * R2, 1}, CMat{T, (i64)x1 * cp, 1},
-           OMat(mm, n, (i64)x1 * n * cp, cp, cp, (i64)n * cp, 1), R1 * n, x1 * cp, n * R2, 1.0,
-           0.0);
+      {
+        const OMat om(mm, n, (i64)x1 * n * cp, cp, cp, (i64)n * cp, 1);
+        const SpOp S = build_spop(c, acore(c, i), R1, n, n, R2, SP_P);
+        if (c.status) return 0.0;
+        if (S.rows)
+          spmm(c, S, T, (i64)x1 * cp, 1, om, x1 * cp, 1.0, 0.0);
+        else
+          gemm(c, CMat{acore(c, i), (i64)n * R2, 1}, CMat{T, (i64)x1 * cp, 1}, om, R1 * n,
+               x1 * cp, n * R2, 1.0, 0.0);
+      }
       // b rows (the first core: the same row, accumulated), sign as in
       // residual_train_core
       const int kb = c.T->b_orth_center >= 0 ? c.T->b_orth_center : 0;
@@ -1304,31 +1536,10 @@ __device__ __noinline__ bool over_time(Ctx& c, unsigned long long t_start) {
 // the kernel
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(TTB_THREADS, 1)
-    k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
-  extern __shared__ double dyn[];
-  __shared__ Sm sm;
-  double* pool = dyn + GSTAGES * GSTAGE_D;
-  const ttb_amen_task_t* T = tasks + blockIdx.x;
-  Ctx c;
-  c.T = T;
-  c.sm = &sm;
-  c.slab = T->slab;
-  c.cap = T->slab_doubles;
-  c.top = 0;
-  c.pool = pool;
-  c.ring = dyn;
-  c.gsm = reinterpret_cast<GemmSmem*>(dyn);
-  c.d = T->d;
-  c.rmax = rmax;
-  c.K = T->kickrank;
-  c.status = ST_OK;
-  c.flops = 0.0;
-  c.applies = 0;
-  c.check = 0.0;
-  c.check_qr = 0.0;
-  c.n_qr2 = 0;
-  for (int i = 0; i < PH_N; ++i) c.cyc[i] = 0;
+// The whole solve of one task (everything but the tensor-memory set-up).
+__device__ __noinline__ void amen_run(Ctx& c, int rmax) {
+  Sm& sm = *c.sm;
+  const ttb_amen_task_t* T = c.T;
   const unsigned long long t_start = global_ns();
   long long t_ph = clock64();
 #define PHASE(ph)                         \
@@ -1580,6 +1791,54 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
 #undef CHECK
 }
 
+// The tensor pipeline's shared-memory stages take the start of the pool,
+// which the factorisations use only outside the mixed-precision solves.
+static_assert(TC_RING_BYTES <= kPoolBytes, "tensor-core stages must fit the pool");
+
+__global__ void __launch_bounds__(TTB_THREADS, 1)
+    k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
+  extern __shared__ __align__(16) double dyn[];
+  __shared__ Sm sm;
+  double* pool = dyn + GSTAGES * GSTAGE_D;
+  const ttb_amen_task_t* T = tasks + blockIdx.x;
+  Ctx c;
+  c.T = T;
+  c.sm = &sm;
+  c.slab = T->slab;
+  c.cap = T->slab_doubles;
+  c.top = 0;
+  c.pool = pool;
+  c.ring = dyn;
+  c.gsm = reinterpret_cast<GemmSmem*>(dyn);
+  c.d = T->d;
+  c.rmax = rmax;
+  c.K = T->kickrank;
+  c.status = ST_OK;
+  c.flops = 0.0;
+  c.applies = 0;
+  c.check = 0.0;
+  c.check_qr = 0.0;
+  c.n_qr2 = 0;
+  for (int i = 0; i < PH_N; ++i) c.cyc[i] = 0;
+  c.mixed = (T->precision == 1);
+  c.flops_tc = 0.0;
+  c.refine = 0;
+  if (c.mixed) {
+    c.tc.ring = reinterpret_cast<float*>(pool);
+    c.tc.mbar = sm.mbar;
+    c.tc.slot = &sm.tmem_slot;
+    tc_init(c.tc);
+  }
+  amen_run(c, rmax);
+  if (c.mixed) {
+    tc_release(c.tc);
+    if (threadIdx.x == 0) {
+      T->residuals[2 * T->max_sweeps + 14] = c.flops_tc;
+      T->residuals[2 * T->max_sweeps + 15] = (double)c.refine;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1610,8 +1869,10 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   // stack bound of one sweep step: b_loc, u and z_new, then the largest of
   // the sub-steps, each term rounded up generously
   const long long r = rmax, n = nmax, R = Rmax, N = r * n * r, cols = r + K;
-  const long long env = 2 * r * R * n * r + r * n * r;
-  const long long apply = 2 * r * n * R * r + R * n * n * R + R * r * r;  // + permute_op
+  // sparse forms of an operator core (two in permute_op, one elsewhere)
+  const long long sp = spop_doubles(R * n * n * R, R * n);
+  const long long env = 2 * r * R * n * r + r * n * r + sp;
+  const long long apply = 2 * r * n * R * r + R * n * n * R + R * r * r + 2 * sp;  // + permute_op
   const long long dn = std::min<long long>(direct_solve_size, N);
   const long long direct = dn * dn + dn;
   const long long iter = N + 6 * N + apply;
@@ -1622,7 +1883,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
                          + r * n * cols + cols * cols + cols * n * r  // Q, R, next
                          + r * n * cols + cols + r * n * K;            // qr work, block
   const long long bb = R * r + rbmax;
-  const long long resid = 2 * bb * bb + bb * n * bb + bb * n * bb + bb * bb;
+  const long long resid = 2 * bb * bb + bb * n * bb + bb * n * bb + bb * bb + sp;
   const long long step = 3 * N + K * n * K +
                          std::max({env, direct, iter, rank + fact, resid, 2 * rbmax * n * r});
   return slots + 2 * step + (1 << 16);

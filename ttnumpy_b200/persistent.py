@@ -57,7 +57,7 @@ def _orth(t) -> Optional[int]:
 
 
 STATUS = {0: "ok", -1: "singular local system", -3: "slab too small", -4: "rank above rmax",
-          -5: "unsupported settings", -6: "time limit"}
+          -5: "unsupported settings", -6: "time limit", -7: "tensor-core pipeline gave up"}
 
 
 @dataclass
@@ -65,6 +65,10 @@ class Result:
     x: Optional[TensorTrain]
     info: SolverInfo
     status: int
+    device_ms: float = 0.0  # the block's run time on the device for this solve
+    flops: float = 0.0      # FLOPs of its float64 dense and sparse products
+    flops_tc: float = 0.0   # FLOPs of its 3xTF32 tensor-core products (mixed precision)
+    refine: int = 0         # float64 refinement steps of its local solves (mixed precision)
 
 
 class _Prepared:
@@ -79,6 +83,12 @@ class _Prepared:
         seed = kw.pop("seed", None)
         return_info = kw.pop("return_info", True)
         kw.pop("inplace", None)
+        # persistent-engine option (not an argument of the reference's amen):
+        # "fp64", or "mixed" for 3xTF32 inner solves with float64 refinement
+        precision = kw.pop("precision", "fp64")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.precision = precision
         if kick <= 0:
             raise ValueError(f"kickrank must be a positive integer, got {kick}")
         if max_rank is not None and max_rank <= 0:
@@ -119,6 +129,29 @@ class _Prepared:
         self.d = d
         self.modes = modes
 
+    def packed(self) -> np.ndarray:
+        """Operator, right-hand side, initial guess and residual start, core
+        after core, as one float64 vector (the layout a task reads)."""
+        return np.concatenate([c.reshape(-1) for cores in (self.A, self.b, self.x0, self.z0)
+                               for c in cores])
+
+    def offsets(self) -> np.ndarray:
+        """Start of every core in :meth:`packed` (A, b, x0, z0 cores in order)."""
+        sizes = [c.size for cores in (self.A, self.b, self.x0, self.z0) for c in cores]
+        return np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+
+    def resident(self):
+        """This request's inputs on the device (uploaded on the first call
+        and kept): (packed cores, their offsets)."""
+        if getattr(self, "_dev", None) is None:
+            host = torch.from_numpy(self.packed()).pin_memory()
+            self._dev = (host.to("cuda", non_blocking=True),
+                         torch.from_numpy(self.offsets()).to("cuda", non_blocking=True))
+        return self._dev
+
+    def drop_resident(self) -> None:
+        self._dev = None
+
     def dims(self) -> np.ndarray:
         d = self.d
         R = [c.shape[0] for c in self.A] + [1]
@@ -150,22 +183,37 @@ class PersistentBatch:
     """
 
     def __init__(self, preps: List["_Prepared"], rmax: int, debug: bool = False,
-                 time_limit: Optional[float] = None):
+                 time_limit: Optional[float] = None, resident: bool = False):
         lib = _lib_handle()
         self.preps, self.rmax = preps, rmax
         n = len(preps)
-        blocks, offs = [], []
-        pos = 0
-        for p in preps:
-            for cores in (p.A, p.b, p.x0, p.z0):
-                for c in cores:
-                    offs.append(pos)
-                    blocks.append(c.reshape(-1))
-                    pos += c.size
-        host = np.concatenate(blocks) if blocks else np.zeros(1)
-        self.h2d_bytes = host.nbytes
-        self.dev_in = torch.from_numpy(host).pin_memory().to("cuda", non_blocking=True)
-        self.dev_off = torch.from_numpy(np.asarray(offs, dtype=np.int64)).to("cuda")
+        # inputs: per request already on the device (``resident``: uploaded
+        # beforehand by _Prepared.resident), or packed here into one buffer
+        # and copied from host memory
+        if resident:
+            devs = [p.resident() for p in preps]
+            in_ptr = [d[0].data_ptr() for d in devs]
+            off_ptr = [d[1].data_ptr() for d in devs]
+            self.h2d_bytes = 0
+            self.dev_in = self.dev_off = None
+            self._resident = devs  # keeps the buffers alive with the batch
+        else:
+            host = np.concatenate([p.packed() for p in preps])
+            offs = []
+            pos = 0
+            for p in preps:
+                offs.append(p.offsets() + pos)
+                pos += sum(c.size for cores in (p.A, p.b, p.x0, p.z0) for c in cores)
+            self.h2d_bytes = host.nbytes
+            self.dev_in = torch.from_numpy(host).pin_memory().to("cuda", non_blocking=True)
+            self.dev_off = torch.from_numpy(np.concatenate(offs)).to("cuda")
+            in_ptr = [self.dev_in.data_ptr()] * n
+            off_ptr = []
+            opos = 0
+            for p in preps:
+                off_ptr.append(self.dev_off.data_ptr() + 8 * opos)
+                opos += 4 * p.d
+            self._resident = None
         dims_host = [p.dims() for p in preps]
         dim_pos = np.cumsum([0] + [len(x) for x in dims_host])
         self.dev_dims = torch.from_numpy(np.concatenate(dims_host)).to("cuda")
@@ -174,23 +222,17 @@ class PersistentBatch:
         self.slabs = torch.empty(int(self.slab_pos[-1]), dtype=torch.float64, device="cuda")
         self.dmax = max(p.d for p in preps)
         smax = max(max(p.st.max_sweeps for p in preps), 1)
-        self.resid = torch.zeros(n, 2 * smax + 14, dtype=torch.float64, device="cuda")
+        self.resid = torch.zeros(n, 2 * smax + 16, dtype=torch.float64, device="cuda")
         self.result = torch.zeros(n, 6 + self.dmax, dtype=torch.int32, device="cuda")
         self.xoff = torch.zeros(n, self.dmax, dtype=torch.int64, device="cuda")
         tasks = (Task * n)()
-        base_in, base_off = self.dev_in.data_ptr(), self.dev_off.data_ptr()
         # blocks start in task order: longest solves first (estimated cost)
         self.order = sorted(range(n), key=lambda i: -_cost(preps[i]))
         slot = {i: j for j, i in enumerate(self.order)}
-        opos = 0
         for i, p in enumerate(preps):
             t = tasks[slot[i]]
-            ptrs = []
-            for _ in range(4):
-                ptrs.append(base_off + 8 * opos)
-                opos += p.d
-            t.A = t.b = t.x0 = t.z0 = base_in
-            t.A_off, t.b_off, t.x0_off, t.z0_off = ptrs
+            t.A = t.b = t.x0 = t.z0 = in_ptr[i]
+            t.A_off, t.b_off, t.x0_off, t.z0_off = [off_ptr[i] + 8 * j * p.d for j in range(4)]
             t.dims = self.dev_dims.data_ptr() + 4 * int(dim_pos[i])
             t.slab = self.slabs.data_ptr() + 8 * int(self.slab_pos[i])
             t.slab_doubles = sizes[i]
@@ -218,6 +260,7 @@ class PersistentBatch:
             t.truncation_tol = st.truncation_tol or 0.0
             t.debug = int(debug)
             t.time_limit_ns = int(time_limit * 1e9) if time_limit else 0
+            t.precision = 1 if p.precision == "mixed" else 0
         raw = np.frombuffer(bytes(tasks), dtype=np.uint8)
         self.dev_tasks = torch.from_numpy(raw.copy()).to("cuda")
 
@@ -274,11 +317,15 @@ class PersistentBatch:
         for i, p in enumerate(self.preps):
             status = int(res_h[i, 0])
             info = SolverInfo()
+            hb = 2 * p.st.max_sweeps
+            dev_ms = (resid_h[i, hb + 11] - resid_h[i, hb + 10]) * 1e-6
+            flops = float(resid_h[i, hb])
+            extra = dict(flops_tc=float(resid_h[i, hb + 14]), refine=int(resid_h[i, hb + 15]))
             if status == -6:  # time limit: the sweeps completed before it
                 info.num_sweeps_run = int(res_h[i, 1])
                 info.residuals = [float(v) for v in resid_h[i, :info.num_sweeps_run]]
             if status != 0:
-                out.append(Result(None, info, status))
+                out.append(Result(None, info, status, dev_ms, flops, **extra))
                 continue
             sweeps = int(res_h[i, 1])
             info.num_sweeps_run = sweeps
@@ -298,7 +345,8 @@ class PersistentBatch:
                 size = bonds[k] * p.modes[k] * bonds[k + 1]
                 cores.append(self.slabs[o:o + size].view(bonds[k], p.modes[k], 1,
                                                          bonds[k + 1]).clone())
-            out.append(Result(TensorTrain._wrap(cores, orth_center=0), info, status))
+            out.append(Result(TensorTrain._wrap(cores, orth_center=0), info, status, dev_ms,
+                              flops, **extra))
         return out
 
     def run(self, stream: Optional[torch.cuda.Stream] = None) -> List[Result]:
@@ -317,6 +365,18 @@ class PersistentBatch:
         their cores were cloned out of the slabs)."""
         self.dev_in = self.dev_off = self.dev_dims = self.slabs = None
         self.resid = self.result = self.xoff = None
+        self._resident = None
+
+
+def initial_rmax(p: "_Prepared") -> int:
+    """Slot capacity a request starts with: bonds of solutions on mode-2
+    (QTT) trains stay far below 32, those of mode sizes up to 32 below 64,
+    and larger modes reach the 70s at residual 1e-8, where starting at 64
+    would cost a full re-run at twice the capacity."""
+    n = max(p.modes)
+    if n <= 4:
+        return 32
+    return 64 if n < 64 else 96
 
 
 def _cost(p: "_Prepared") -> float:

@@ -10,8 +10,10 @@ does not wait for the longest solve of an earlier batch.  Each launch copies
 its requests' inputs from host memory on its own stream and the solutions
 are read back when its completion event has fired.
 
-A request whose bonds outgrow the launch's slot capacity (status -4) is
-queued again with twice the capacity, as ``amen_persistent`` does.
+Each request starts at a slot capacity chosen from its mode sizes
+(``initial_rmax``); one whose bonds outgrow it (status -4) is queued again
+with twice the capacity, as ``amen_persistent`` does.  A launch takes
+requests of one capacity, that of the oldest waiting request.
 
 Requests are admitted by device memory: with ``mem_budget`` set, a launch
 takes waiting requests only while the work areas (slabs) of all launches in
@@ -31,7 +33,7 @@ from typing import Callable, List, Optional, Sequence
 import torch
 
 from . import kernels as K
-from .persistent import PersistentBatch, Result, _cost, _Prepared, slab_doubles
+from .persistent import PersistentBatch, Result, _cost, _Prepared, initial_rmax, slab_doubles
 
 
 def admit(sizes: Sequence[int], room: Optional[int], idle: bool) -> List[int]:
@@ -81,9 +83,9 @@ class PersistentServer:
     a launch.
     """
 
-    def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: int = 64,
+    def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: Optional[int] = None,
                  max_rmax: int = 256, min_interval: float = 0.005, download: bool = True,
-                 mem_budget: Optional[int] = None):
+                 mem_budget: Optional[int] = None, resident: bool = False):
         K.device_ok()
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.free = list(range(streams))
@@ -93,6 +95,7 @@ class PersistentServer:
         self.min_interval = min_interval
         self.download = download
         self.mem_budget = mem_budget
+        self.resident = resident  # inputs uploaded before submission (no copy per launch)
         self.inflight_bytes = 0
         self.peak_bytes = 0
         self.queue: List[Job] = []
@@ -105,7 +108,12 @@ class PersistentServer:
 
     def submit(self, rid: int, arrival: float, A, b, x0=None, kwargs: Optional[dict] = None) -> Job:
         """Validate a request on the host and queue it (``amen`` arguments)."""
-        job = Job(rid, arrival, _Prepared(A, b, x0, dict(kwargs or {})), self.rmax)
+        return self.submit_prepared(rid, arrival, _Prepared(A, b, x0, dict(kwargs or {})))
+
+    def submit_prepared(self, rid: int, arrival: float, prep: _Prepared) -> Job:
+        """Queue an already validated request; it starts at the server's
+        slot capacity, or at ``initial_rmax`` for its mode sizes."""
+        job = Job(rid, arrival, prep, self.rmax or initial_rmax(prep))
         job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
         self.queue.append(job)
         return job
@@ -115,7 +123,9 @@ class PersistentServer:
             return False
         if len(self.queue) < self.max_batch and now - self._last_launch < self.min_interval:
             return False
-        rmax = min(j.rmax for j in self.queue)
+        # one slot capacity per launch: the oldest waiting request's, so that
+        # requests of every capacity are launched in arrival order
+        rmax = self.queue[0].rmax
         take = [j for j in self.queue if j.rmax == rmax][: self.max_batch]
         room = None if self.mem_budget is None else self.mem_budget - self.inflight_bytes
         idx = admit([j.slab_bytes for j in take], room, not self.inflight)
@@ -128,7 +138,7 @@ class PersistentServer:
         si = self.free.pop()
         s = self.streams[si]
         with torch.cuda.stream(s):
-            batch = PersistentBatch([j.prep for j in take], rmax)
+            batch = PersistentBatch([j.prep for j in take], rmax, resident=self.resident)
             batch.launch(s)
             ev = torch.cuda.Event()
             ev.record(s)
@@ -183,9 +193,10 @@ class PersistentServer:
 
     def serve(self, requests: Sequence, arrivals: Sequence[float],
               clock: Callable[[], float] = time.perf_counter) -> List[Job]:
-        """Submit ``requests`` [(A, b, x0, kwargs)] at ``arrivals`` (seconds
-        from the start) and serve them to completion; returns the jobs in
-        request order."""
+        """Submit ``requests`` [(A, b, x0, kwargs)], or requests already
+        prepared (``_Prepared``), at ``arrivals`` (seconds from the start) and
+        serve them to completion; returns the jobs in request order.
+        Requests arriving at the same time are queued in the order given."""
         order = sorted(range(len(requests)), key=lambda i: arrivals[i])
         jobs: List[Optional[Job]] = [None] * len(requests)
         t0 = clock()
@@ -194,8 +205,11 @@ class PersistentServer:
             now = clock() - t0
             while nxt < len(order) and arrivals[order[nxt]] <= now:
                 i = order[nxt]
-                A, b, x0, kw = requests[i]
-                jobs[i] = self.submit(i, arrivals[i], A, b, x0, kw)
+                if isinstance(requests[i], _Prepared):
+                    jobs[i] = self.submit_prepared(i, arrivals[i], requests[i])
+                else:
+                    A, b, x0, kw = requests[i]
+                    jobs[i] = self.submit(i, arrivals[i], A, b, x0, kw)
                 nxt += 1
             if not self.step(clock() - t0):
                 time.sleep(0.0005)

@@ -252,35 +252,69 @@ def random_tt(modes: Sequence[int], rank: int, seed: int) -> List[np.ndarray]:
     return [rng.random((ranks[i], modes[i], 1, ranks[i + 1])) for i in range(d)]
 
 
-def serving_stream(count: int, rate: float, seed: int = 0, large_share: float = 0.1,
-                   large_d: int = 24, large_n: int = 64, large_rank: int = 8):
-    """Request stream: Poisson arrivals at ``rate`` per second.
+def large_diffusion(theta: np.ndarray, rhs_seed: int, n: int = 64, rank: int = 8) -> Problem:
+    """The large request class: parametric diffusion in ``d = len(theta)``
+    dimensions with mode size ``n`` and a random rank-``rank`` right-hand
+    side (``random_tt`` with seed ``rhs_seed``)."""
+    d = len(theta)
+    A = diffusion_operator(d, n, theta, diffusion_scale(d))
+    b = random_tt([n] * d, rank, seed=rhs_seed)
+    return Problem(f"large_d{d}_n{n}", A, b, meta={"kind": "large", "d": d, "n": n})
 
-    Each request is, with probability ``large_share``, a large diffusion
-    solve (``d = large_d``, ``n = large_n``, right-hand side a random
-    rank-``large_rank`` train); otherwise, with equal odds, a parametric
-    diffusion draw or a 2-D QTT Poisson problem with ``2N`` cores,
-    ``N ~ U{3..10}``.  Yields ``(arrival_time, Problem)``.
-    """
+
+#: Shares of the serving mix: large requests, then diffusion and QTT
+#: Poisson in equal parts of the rest.
+LARGE_SHARE = 0.1
+
+
+def serving_request(rng: np.random.Generator, large_share: float = LARGE_SHARE,
+                    large_d: int = 24, large_n: int = 64, large_rank: int = 8,
+                    dims=(4, 12), modes=(16, 32, 64), levels=(3, 10)) -> Problem:
+    """One request of the serving mix, drawn from ``rng``: with probability
+    ``large_share`` a large diffusion solve (``d = large_d``, ``n =
+    large_n``, random rank-``large_rank`` right-hand side); otherwise, with
+    equal odds, a parametric diffusion draw (``d ~ U{dims}``, ``n ~
+    U(modes)``, ``theta ~ U(-1, 1)``) or a 2-D QTT Poisson problem with
+    ``2N`` cores, ``N ~ U{levels}``.  ``meta["kind"]`` names the class."""
+    u = rng.random()
+    if u < large_share:
+        theta = rng.uniform(-1.0, 1.0, size=large_d)
+        return large_diffusion(theta, int(rng.integers(1 << 31)), large_n, large_rank)
+    if u < large_share + (1 - large_share) / 2:
+        d = int(rng.integers(dims[0], dims[1] + 1))
+        n = int(rng.choice(modes))
+        p = parametric_diffusion(d, n, rng.uniform(-1.0, 1.0, size=d))
+        p.meta["kind"] = "diffusion"
+        return p
+    N = int(rng.integers(levels[0], levels[1] + 1))
+    base = _qtt_poisson_cached(N)
+    return Problem(base.name, base.A, base.b, meta={"kind": "qtt", "levels": N})
+
+
+_QTT_CACHE: dict = {}
+
+
+def _qtt_poisson_cached(levels: int) -> Problem:
+    """``qtt_poisson_2d(levels)`` built once per level (the TT-SVD of the
+    right-hand side dominates building a request); requests share its
+    read-only core arrays."""
+    if levels not in _QTT_CACHE:
+        _QTT_CACHE[levels] = qtt_poisson_2d(levels)
+    return _QTT_CACHE[levels]
+
+
+def serving_requests(count: int, seed: int = 0, **kw) -> List[Problem]:
+    """``count`` requests of the serving mix from one generator seeded
+    ``seed`` (see ``serving_request`` for the classes and keywords)."""
     rng = np.random.default_rng(seed)
-    t = 0.0
-    out = []
-    for i in range(count):
-        t += float(rng.exponential(1.0 / rate))
-        u = rng.random()
-        if u < large_share:
-            theta = rng.uniform(-1.0, 1.0, size=large_d)
-            A = diffusion_operator(large_d, large_n, theta, diffusion_scale(large_d))
-            b = random_tt([large_n] * large_d, large_rank, seed=int(rng.integers(1 << 31)))
-            p = Problem(f"large_d{large_d}", A, b, meta={"kind": "large"})
-        elif u < large_share + (1 - large_share) / 2:
-            d = int(rng.integers(4, 13))
-            n = int(rng.choice((16, 32, 64)))
-            p = parametric_diffusion(d, n, rng.uniform(-1.0, 1.0, size=d))
-            p.meta["kind"] = "diffusion"
-        else:
-            levels = int(rng.integers(3, 11))
-            p = qtt_poisson_2d(levels)
-            p.meta["kind"] = "qtt"
-        out.append((t, p))
-    return out
+    return [serving_request(rng, **kw) for _ in range(count)]
+
+
+def serving_stream(count: int, rate: float, seed: int = 0, **kw):
+    """Request stream: the requests of ``serving_requests(count, seed)``
+    arriving as a Poisson process at ``rate`` per second (exponential gaps
+    from a second generator seeded ``seed + 1``).  Returns
+    ``[(arrival_time, Problem), ...]``."""
+    reqs = serving_requests(count, seed, **kw)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=count)
+    return list(zip(np.cumsum(gaps).tolist(), reqs))

@@ -26,8 +26,10 @@ to the host inside a sweep; the relative residual comes back once per sweep.
 
 from __future__ import annotations
 
+import contextlib
 import logging
 import math
+import threading
 import time
 from typing import Optional, Tuple, Union
 
@@ -50,6 +52,29 @@ from .common import (
 )
 
 logger = logging.getLogger("ttnumpy")
+
+
+class _TimeLimit(threading.local):
+    seconds: Optional[float] = None
+
+
+_TIME_LIMIT = _TimeLimit()
+
+
+@contextlib.contextmanager
+def solve_time_limit(seconds: Optional[float]):
+    """Within the block, an ``amen`` call on this thread stops after the
+    first sweep that ends more than ``seconds`` after the call started (the
+    per-solve time limit of the reference's benchmark runner,
+    ``benchmarks/poisson.py:95-143``); its ``SolverInfo`` then reports
+    ``max_sweeps`` with the sweeps run so far.  Outside such a block the
+    sweep count alone bounds a solve, as in the reference."""
+    prev = _TIME_LIMIT.seconds
+    _TIME_LIMIT.seconds = seconds
+    try:
+        yield
+    finally:
+        _TIME_LIMIT.seconds = prev
 
 
 def _c3(core: torch.Tensor) -> torch.Tensor:
@@ -488,6 +513,10 @@ def amen(A: TensorTrain, b: TensorTrain, x0: Optional[TensorTrain] = None, inpla
             info.stop_reason = StopReason.STAGNATED
             logger.warning("AMEn stagnated at sweep %d: relative residual %.3e vs %.3e previous",
                            sweep + 1, info.residuals[-1], info.residuals[-2])
+            break
+        limit = _TIME_LIMIT.seconds
+        if limit is not None and time.perf_counter() - started > limit:
+            logger.warning("AMEn stopped at sweep %d by the time limit of %.1fs", sweep + 1, limit)
             break
 
     # amen.py:710-720: bonds above the product of the modes to their left
