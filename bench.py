@@ -18,8 +18,8 @@ the continuous-batching server on the persistent whole-solve kernel
 (``persistent_serving``), and value = solved requests / device time of the
 whole run.  ``e2e``: the same server fed from host memory through its public
 API (inputs copied per launch, solutions read back) with a seeded Poisson
-stream arriving at twice the measured capacity; two more passes at 0.5x and
-0.8x of it report the latency at sustainable load.
+stream arriving at twice the measured capacity; one more pass at 0.8x of it
+(``--serve-loads``) reports the latency at a sustainable load.
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
 (the NumPy/SciPy restatement of the reference path, kept within a few
@@ -66,10 +66,10 @@ def parse(argv=None):
     ap.add_argument("--requests", type=int, default=148,
                     help="requests per step (148 = one per SM of a B200)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--serve-requests", type=int, default=600,
+    ap.add_argument("--serve-requests", type=int, default=400,
                     help="requests in each served pass (a slice of the stream after the "
                          "timed steps' requests)")
-    ap.add_argument("--serve-loads", default="0.5,0.8",
+    ap.add_argument("--serve-loads", default="0.8",
                     help="arrival rates of the latency passes, as fractions of the measured "
                          "capacity (the throughput pass arrives at twice it)")
     ap.add_argument("--serve-mem-gb", type=float, default=96.0,
@@ -396,6 +396,78 @@ def plain_run(reqs, limit, torch):
             "classes": class_stats(kinds, ok)}
 
 
+def config1_problem():
+    """Config 1: the 8-D Laplacian with n = 32 (h = 1/33) and a rank-4
+    uniform right-hand side (tt.rand seed 0)."""
+    from ttnumpy_b200 import problems as P
+
+    return P.Problem("config1", P.laplacian_nd(8, 32), P.random_tt([32] * 8, 4, seed=0),
+                     meta={"kind": "config1"})
+
+
+def config1_run(torch):
+    """Single-solve latency of config 1 (max_sweeps 20): one request alone
+    in a persistent launch (one SM) and the drop-in (the whole GPU)."""
+    import ttnumpy_b200 as tt
+    from ttnumpy_b200.persistent import amen_persistent
+
+    p = config1_problem()
+    kw = dict(residual_tol=TOL, symmetric=True, max_sweeps=20, seed=0, stagnation_factor=None)
+    out = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = amen_persistent([(p.A, p.b, None, kw)], rmax=64)[0]
+    torch.cuda.synchronize()
+    out["persistent_s"] = time.perf_counter() - t0
+    out["persistent_device_s"] = r.device_ms * 1e-3
+    out["persistent"] = {"status": r.status, "sweeps": r.info.num_sweeps_run,
+                         "residual": r.info.residuals[-1] if r.info.residuals else None}
+    t0 = time.perf_counter()
+    x, info = tt.amen(tt.TensorTrain(p.A), tt.TensorTrain(p.b), return_info=True, **kw)
+    torch.cuda.synchronize()
+    out["dropin_s"] = time.perf_counter() - t0
+    out["dropin"] = {"sweeps": info.num_sweeps_run, "residual": info.residuals[-1]}
+    return out
+
+
+def rounding_run(torch, pairs=1024, reps=5):
+    """Config 2: ``(p_i + q_i).truncate(1e-6)`` for 1024 pairs of uniform
+    rank-32 trains with d = 16, n = 4 (seeds 2i, 2i + 1), all pairs in one
+    launch of the batched rounding kernel.  Pairs per second over ``reps``
+    launches (inputs resident), and the relative Frobenius error of a sample
+    of results against the float64 oracle's rounding of the same sums."""
+    from oracle import tt_oracle as O
+    from ttnumpy_b200 import problems as P
+    from ttnumpy_b200.rounding import PackedTrains, RoundPlan
+
+    ps = [P.random_tt([4] * 16, 32, seed=2 * i) for i in range(pairs)]
+    qs = [P.random_tt([4] * 16, 32, seed=2 * i + 1) for i in range(pairs)]
+    pk, qk = PackedTrains.from_numpy(ps), PackedTrains.from_numpy(qs)
+    plan = RoundPlan(pairs, 16, pk.modes, pk.bonds, qk.bonds, pk.offsets, qk.offsets)
+    res = plan.run(pk.data, qk.data, 1e-6, None)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        res = plan.run(pk.data, qk.data, 1e-6, None)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    errs, same = [], 0
+    for i in range(0, pairs, pairs // 8):
+        got = O.Train(res.train(i).to_numpy())
+        want = O.truncate(O.add(O.Train(ps[i]), O.Train(qs[i])), 1e-6)
+        errs.append(O.tt_norm(O.add(got, O.scale(want, -1.0))) / O.tt_norm(want))
+        same += int(list(got.bonds) == list(want.bonds))
+    in_bytes = 8 * (pk.data.numel() + qk.data.numel())
+    return {"workload": "1024 pairs of uniform rank-32 trains, d=16, n=4, summed to rank 64, "
+                        "truncate(1e-6), one launch of ttb_round_batch", "pairs_per_s":
+            pairs / (ms * 1e-3), "ms_per_launch": ms, "input_gb_s": in_bytes / (ms * 1e-3) / 1e9,
+            "sample_rel_err_vs_fp64_oracle_max": max(errs),
+            "sample_bonds_equal": f"{same}/{len(errs)}",
+            "precision": "float64 (no 3xTF32 rounding variant)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -485,6 +557,10 @@ def main():
     plain = None
     if world == 1 and args.plain_sample > 0:
         plain = plain_run(reqs[:args.plain_sample], args.plain_limit, torch)
+    secondary = None
+    if world == 1:
+        secondary = {"config2_rounding": rounding_run(torch), "config1_single_solve":
+                     config1_run(torch)}
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -504,6 +580,10 @@ def main():
     if world == 1:
         n_cpu = args.cpu_sample or 2 * cpu_cores()
         cpu = cpu_baseline(reqs[:n_cpu], cpu_cores(), args.cpu_limit)
+        # config 1 on one host core, uncapped (the secondary single-solve line)
+        dt, conv, _ = cpu_run([config1_problem()], 1, 1e9)[1][0]
+        secondary["config1_single_solve"]["cpu_oracle_s"] = dt
+        secondary["config1_single_solve"]["cpu_oracle_converged"] = conv
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -513,7 +593,7 @@ def main():
             "latency_ms": {"p50": percentile(lats, 50), "p99": percentile(lats, 99)},
             "peak_work_gb": peak_gb,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "plain_gpu": plain, "clocks": clocks.summary()}
+            "plain_gpu": plain, "clocks": clocks.summary(), "secondary": secondary}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

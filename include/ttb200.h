@@ -466,8 +466,8 @@ int ttb_round_batch(const ttb_round_t* problem, void* stream);
  * slab + x_offsets[k].  Blocks start in task order, so listing the longest
  * solves first shortens the launch.  local_rtol > 0
  * selects MINRES for local systems above direct_solve_size unknowns (at
- * most min(5 N, 2000) iterations per call, SciPy's cap being 5 N);
- * local_rtol <= 0 refuses them (status -5).
+ * most min(5 N, 2000) iterations per call, SciPy's cap being 5 N), or
+ * GMRES with local_gmres; local_rtol <= 0 refuses them (status -5).
  * --------------------------------------------------------------------- */
 typedef struct {
   const double* A;
@@ -506,6 +506,9 @@ typedef struct {
                               [2*max_sweeps + 14] receives their FLOPs, [+ 15]
                               the refinement steps; status -7 if a tensor-core
                               wait gave up) */
+  int local_gmres;         /* 1: iterative local solves by restarted GMRES
+                              (symmetric=False; SciPy's gmres, restart 20, at
+                              most 100 restart cycles per call), 0: MINRES */
 } ttb_amen_task_t;
 long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int rmax,
                                 int direct_solve_size);

@@ -84,6 +84,25 @@ def test_golden_cases_one_launch(pers):
         assert len(res.info.max_bonds) == res.info.num_sweeps_run
 
 
+def test_gmres_local_solves(pers):
+    """A non-symmetric system with local solves forced onto GMRES
+    (direct_solve_size 4): the persistent kernel's restarted GMRES against
+    the reference's run."""
+    req, data = golden_request("amen_nonsym_gmres")
+    (res,) = pers.amen_persistent([req])
+    assert res.status == 0, pers.STATUS.get(res.status)
+    A_c, b, _, args = req
+    b_c, b_oc = golden_train(data, "b")
+    host = O.relative_residual(O.Train(A_c), O.Train(b_c, b_oc), otrain(res.x))
+    assert res.info.converged, res.info
+    assert host <= args["residual_tol"] * 1.05
+    assert res.info.residuals[-1] == pytest.approx(host, rel=1e-6, abs=1e-3 * args["residual_tol"])
+    ref = O.Train(golden_train(data, "x")[0])
+    assert rel_tt(otrain(res.x), ref) < 1e-6
+    assert abs(res.info.num_sweeps_run - int(data["num_sweeps_run"])) <= 1
+    assert res.info.local_solves == int(data["local_solves"])
+
+
 def test_threshold_mode_case(pers):
     req, data = golden_request("amen_lap5_threshold")
     (res,) = pers.amen_persistent([req])

@@ -114,7 +114,8 @@ class AmenTask(C.Structure):
                 ("stagnation_on", I), ("x0_orth_center", I), ("b_orth_center", I),
                 ("residual_tol", D), ("error_threshold", D), ("residual_damp", D),
                 ("stagnation_factor", D), ("local_rtol", D), ("truncation_tol", D),
-                ("debug", I), ("time_limit_ns", L), ("precision", I)]
+                ("debug", I), ("time_limit_ns", L), ("precision", I),
+                ("local_gmres", I)]
 
 
 _SIGNATURES = {

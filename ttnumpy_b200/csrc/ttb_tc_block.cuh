@@ -158,23 +158,40 @@ static __device__ __forceinline__ void tc_stage(const CMat& A, const CMat& B, in
   float* alo = st + TC_A_FL;
   float* bhi = st + 2 * TC_A_FL;
   float* blo = st + 2 * TC_A_FL + TC_B_FL;
-  for (int e = threadIdx.x; e < TC_M * TC_K; e += TTB_THREADS) {
+  constexpr int NA = TC_M * TC_K / TTB_THREADS, NB = TC_N * TC_K / TTB_THREADS;
+  static_assert(NA * TTB_THREADS == TC_M * TC_K && NB * TTB_THREADS == TC_N * TC_K,
+                "stage loads must divide evenly");
+  // all of a thread's loads first, so that they are in flight together
+  double xa[NA], xb[NB];
+#pragma unroll
+  for (int t = 0; t < NA; ++t) {
+    const int e = threadIdx.x + t * TTB_THREADS;
     const int u = e >> 5, ln = e & 31;
     const int r = (u % (TC_M / 8)) * 8 + (ln >> 2), c = (u / (TC_M / 8)) * 4 + (ln & 3);
     const int gm = m0 + r, gk = k0 + c;
-    const double x = (gm < M && gk < K) ? A(gm, gk) : 0.0;
-    float hi, lo;
-    tc_split(x, hi, lo);
-    ahi[e] = hi;
-    alo[e] = lo;
+    xa[t] = (gm < M && gk < K) ? A(gm, gk) : 0.0;
   }
-  for (int e = threadIdx.x; e < TC_N * TC_K; e += TTB_THREADS) {
+#pragma unroll
+  for (int t = 0; t < NB; ++t) {
+    const int e = threadIdx.x + t * TTB_THREADS;
     const int u = e >> 5, ln = e & 31;
     const int j = (u % (TC_N / 8)) * 8 + (ln >> 2), c = (u / (TC_N / 8)) * 4 + (ln & 3);
     const int gn = n0 + j, gk = k0 + c;
-    const double x = (gn < N && gk < K) ? B(gk, gn) : 0.0;
+    xb[t] = (gn < N && gk < K) ? B(gk, gn) : 0.0;
+  }
+#pragma unroll
+  for (int t = 0; t < NA; ++t) {
+    const int e = threadIdx.x + t * TTB_THREADS;
     float hi, lo;
-    tc_split(x, hi, lo);
+    tc_split(xa[t], hi, lo);
+    ahi[e] = hi;
+    alo[e] = lo;
+  }
+#pragma unroll
+  for (int t = 0; t < NB; ++t) {
+    const int e = threadIdx.x + t * TTB_THREADS;
+    float hi, lo;
+    tc_split(xb[t], hi, lo);
     bhi[e] = hi;
     blo[e] = lo;
   }

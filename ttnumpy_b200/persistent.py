@@ -8,8 +8,9 @@ reads back the bonds, stop reasons and residual histories.  A solve whose
 bonds outgrow the slot capacity ``rmax`` is re-run with a larger one.
 
 Argument semantics, validation and the ``SolverInfo`` produced are those of
-``amen`` (``ttnumpy/solvers/amen.py:395-725``); MINRES (``symmetric=True``)
-or direct local solves only -- GMRES requests belong to the lockstep engine.
+``amen`` (``ttnumpy/solvers/amen.py:395-725``): direct local solves up to
+``direct_solve_size`` unknowns, MINRES (``symmetric=True``) or restarted
+GMRES beyond.
 """
 
 from __future__ import annotations
@@ -254,9 +255,9 @@ class PersistentBatch:
             t.error_threshold = p.eth
             t.residual_damp = p.damp
             t.stagnation_factor = st.stagnation_factor or 0.0
-            # MINRES tolerance; GMRES-only settings refuse iterative local solves
-            t.local_rtol = ((st.local_rtol or 0.0) if st.iterative_solver is LocalSolver.MINRES
-                            else -1.0)
+            # MINRES (symmetric) or restarted GMRES local solves at local_rtol
+            t.local_rtol = st.local_rtol or 0.0
+            t.local_gmres = int(st.iterative_solver is LocalSolver.GMRES)
             t.truncation_tol = st.truncation_tol or 0.0
             t.debug = int(debug)
             t.time_limit_ns = int(time_limit * 1e9) if time_limit else 0
