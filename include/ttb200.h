@@ -514,6 +514,17 @@ long long ttb_amen_slab_doubles(int d, const int* host_dims, int kickrank, int r
                                 int direct_solve_size);
 int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream);
 
+/* The same solves with a cluster of ``cluster`` (2..8) thread blocks per
+ * task (no counterpart in the reference, which solves on one host thread):
+ * block 0 runs the solve and the other blocks of its cluster compute shares
+ * of its larger dense products and sparse operator-core products, each
+ * output tile or row exactly as a lone block computes it, so the results are
+ * bitwise those of ttb_amen_persistent; the wall time of a large solve
+ * drops, at the price of blocks that idle through its other steps.
+ * cluster <= 1 is ttb_amen_persistent. */
+int ttb_amen_persistent_cluster(const ttb_amen_task_t* tasks, int count, int rmax, int cluster,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,6 +136,20 @@ def test_alone_equals_in_launch(pers):
         assert res <= 1.05e-8
 
 
+def test_cluster_equals_lone_block(pers):
+    """A solve on a cluster of four blocks (the leader's larger products
+    shared out by output tile and row) gives the lone block's bits."""
+    kw = dict(residual_tol=1e-8, symmetric=True, max_sweeps=6, seed=0, stagnation_factor=None)
+    probs = [_diffusion(8, 4, 64), _diffusion(10, 5, 32), P.qtt_poisson_2d(6)]
+    reqs = [(p.A, p.b, None, kw) for p in probs]
+    lone = pers.amen_persistent(reqs, rmax=96)
+    clus = pers.amen_persistent(reqs, rmax=96, cluster=4)
+    for p, a, b in zip(probs, lone, clus):
+        assert a.status == 0 and b.status == 0, (p.name, b.status)
+        assert a.info.residuals == b.info.residuals, p.name
+        assert all(np.array_equal(u, v) for u, v in zip(a.x.to_numpy(), b.x.to_numpy())), p.name
+
+
 def test_matches_dropin(pers):
     import ttnumpy_b200 as tt
 

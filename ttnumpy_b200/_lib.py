@@ -155,6 +155,7 @@ _SIGNATURES = {
     "ttb_round_batch": ([C.POINTER(Round), P], I),
     "ttb_amen_slab_doubles": ([I, C.POINTER(C.c_int), I, I, I], L),
     "ttb_amen_persistent": ([P, I, I, P], I),
+    "ttb_amen_persistent_cluster": ([P, I, I, I, P], I),
 }
 
 _lib = None

@@ -8,6 +8,7 @@
 // when the matrix fits and fall back to the blocked global-memory variants
 // otherwise.  All control flow is uniform across the block: every decision
 // derives from block-wide reductions that all threads see identically.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -75,6 +76,9 @@ struct Ctx {
   long long cyc[8];       // SM cycles per phase (see PH_*)
   int mixed;              // 3xTF32 inner solves with float64 refinement
   TcState tc;             // the block's tensor-core pipeline (mixed only)
+  int csize;              // blocks in the solve's cluster (1: the block alone)
+  struct ClusterCmd* cmd; // the leader's command slot (csize > 1)
+  double* vpart;          // this block's chunk sums of a shared vector pass
   double flops_tc;        // FLOPs of the tensor-core products
   long long refine;       // float64 refinement steps of the local solves
 };
@@ -129,12 +133,206 @@ __device__ double vnorm_diff(const double* x, const double* y, i64 n, double* re
   return sqrt(block_sum(s, red));
 }
 
+// ---------------------------------------------------------------------------
+// products shared out between the blocks of a cluster
+// ---------------------------------------------------------------------------
+
+// A solve may run on a cluster of blocks: block 0 (the leader) runs the
+// whole solve as a lone block would, and posts each product large enough
+// (a tiled GEMM of two or more output tiles, a sparse operator-core product)
+// as a command in its shared memory; the other blocks read it over
+// distributed shared memory and compute their share of the output tiles
+// (tiles rank, rank + csize, ...) or rows, each exactly as the lone block
+// computes it, so the solve's results do not depend on the cluster size.  A
+// command is bracketed by two cluster barriers (posted; done); the leader
+// ends every solve, normally or on an error, with the exit command.
+enum { CL_EXIT = 0, CL_GEMM = 1, CL_SPMM = 2, CL_VEC = 3 };
+
+// The element-wise passes of a MINRES iteration on long vectors run in
+// kVecChunks fixed chunks, each reduced by one block-wide sum; the chunk
+// partials are added in chunk order.  A lone block walks the chunks in turn,
+// a cluster's blocks take chunks rank, rank + csize, ..., so the sums are
+// the same bits either way.  Shorter vectors take one pass by one block.
+constexpr int kVecChunks = 16;
+constexpr i64 kVecChunkMin = 1 << 16;
+enum { VP_SCALE = 0, VP_LANCZOS = 1, VP_RESID = 2, VP_UPDATE = 3 };
+struct VecArgs {
+  int op, first;
+  double a0, a1, a2, a3;
+  double *p0, *p1, *p2, *p3;
+  i64 N;
+};
+
+// One chunk of a pass (pairs of doubles; the odd last element goes to the
+// last chunk); returns the chunk's sum, the same on every thread.
+//   VP_SCALE:   p0 = a0 p1                         (v = r2 / beta)
+//   VP_LANCZOS: p0 -= a0 p1 unless first; sum p2 . p0   (y, r1, v)
+//   VP_RESID:   p0 = p1 - a0 p2; sum p0 . p0        (r1 <- y - g r2)
+//   VP_UPDATE:  p0 <- (p2 - a0 p0 - a1 p1) a2; p3 += a3 p0; sum p3 . p3
+//               (w2 <- new w from v, w2, w; x += phi w)
+__device__ __noinline__ double vpass_chunk(const VecArgs& q, int chunk, double* red) {
+  const i64 N2 = q.N >> 1;
+  const i64 cs = (N2 + kVecChunks - 1) / kVecChunks;
+  const i64 lo = min((i64)chunk * cs, N2), hi = min(lo + cs, N2);
+  const bool tail = (q.N & 1) && chunk == kVecChunks - 1 && threadIdx.x == 0;
+  double acc = 0.0;
+  switch (q.op) {
+    case VP_SCALE: {
+      const double2* R = reinterpret_cast<const double2*>(q.p1);
+      double2* V = reinterpret_cast<double2*>(q.p0);
+#pragma unroll 4
+      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
+        const double2 a = R[i];
+        V[i] = make_double2(q.a0 * a.x, q.a0 * a.y);
+      }
+      if (tail) q.p0[q.N - 1] = q.a0 * q.p1[q.N - 1];
+      break;
+    }
+    case VP_LANCZOS: {
+      double2* Y = reinterpret_cast<double2*>(q.p0);
+      const double2* R1 = reinterpret_cast<const double2*>(q.p1);
+      const double2* V = reinterpret_cast<const double2*>(q.p2);
+#pragma unroll 4
+      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
+        double2 yy = Y[i];
+        const double2 vv = V[i];
+        if (!q.first) {
+          const double2 rr = R1[i];
+          yy.x -= q.a0 * rr.x;
+          yy.y -= q.a0 * rr.y;
+          Y[i] = yy;
+        }
+        acc = fma(vv.x, yy.x, acc);
+        acc = fma(vv.y, yy.y, acc);
+      }
+      if (tail) {
+        double yi = q.p0[q.N - 1];
+        if (!q.first) {
+          yi -= q.a0 * q.p1[q.N - 1];
+          q.p0[q.N - 1] = yi;
+        }
+        acc = fma(q.p2[q.N - 1], yi, acc);
+      }
+      break;
+    }
+    case VP_RESID: {
+      double2* O = reinterpret_cast<double2*>(q.p0);
+      const double2* Y = reinterpret_cast<const double2*>(q.p1);
+      const double2* R2 = reinterpret_cast<const double2*>(q.p2);
+#pragma unroll 4
+      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
+        const double2 yy = Y[i], rr = R2[i];
+        const double2 nv = make_double2(yy.x - q.a0 * rr.x, yy.y - q.a0 * rr.y);
+        O[i] = nv;
+        acc = fma(nv.x, nv.x, acc);
+        acc = fma(nv.y, nv.y, acc);
+      }
+      if (tail) {
+        const double yi = q.p1[q.N - 1] - q.a0 * q.p2[q.N - 1];
+        q.p0[q.N - 1] = yi;
+        acc = fma(yi, yi, acc);
+      }
+      break;
+    }
+    default: {
+      double2* W2 = reinterpret_cast<double2*>(q.p0);
+      const double2* W = reinterpret_cast<const double2*>(q.p1);
+      const double2* V = reinterpret_cast<const double2*>(q.p2);
+      double2* X = reinterpret_cast<double2*>(q.p3);
+#pragma unroll 4
+      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
+        const double2 a1 = W2[i], a2 = W[i], vv = V[i];
+        double2 xx = X[i];
+        const double2 wn = make_double2((vv.x - q.a0 * a1.x - q.a1 * a2.x) * q.a2,
+                                        (vv.y - q.a0 * a1.y - q.a1 * a2.y) * q.a2);
+        W2[i] = wn;
+        xx.x += q.a3 * wn.x;
+        xx.y += q.a3 * wn.y;
+        X[i] = xx;
+        acc = fma(xx.x, xx.x, acc);
+        acc = fma(xx.y, xx.y, acc);
+      }
+      if (tail) {
+        const double wn = (q.p2[q.N - 1] - q.a0 * q.p0[q.N - 1] - q.a1 * q.p1[q.N - 1]) * q.a2;
+        q.p0[q.N - 1] = wn;
+        const double xi = q.p3[q.N - 1] + q.a3 * wn;
+        q.p3[q.N - 1] = xi;
+        acc = fma(xi, xi, acc);
+      }
+      break;
+    }
+  }
+  return block_sum(acc, red);
+}
+
+struct ClusterCmd {
+  int op;
+  VecArgs vec;
+  const double* a;
+  i64 a_rs, a_cs;
+  const double* b;
+  i64 b_rs, b_cs;
+  double* c;
+  i64 c_rs, c_cs, c_rs_hi, c_cs_hi;
+  int c_rdiv, c_cdiv;
+  int M, N, K;
+  double alpha, beta;
+  const int* sp_ptr;
+  const int* sp_col;
+  const double* sp_val;
+  int sp_rows;
+};
+
+__device__ __forceinline__ void cluster_barrier() {
+  cooperative_groups::this_cluster().sync();  // arrive.release + wait.acquire
+  asm volatile("fence.acq_rel.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ OMat cmd_out(const ClusterCmd& q) {
+  return OMat(q.c, q.c_rdiv, q.c_rs_hi, q.c_rs, q.c_cdiv, q.c_cs_hi, q.c_cs);
+}
+
+__device__ void cmd_set_out(ClusterCmd& q, const OMat& C) {
+  q.c = C.p;
+  q.c_rs = C.rs;
+  q.c_cs = C.cs;
+  q.c_rs_hi = C.rs_hi;
+  q.c_cs_hi = C.cs_hi;
+  q.c_rdiv = C.rdiv;
+  q.c_cdiv = C.cdiv;
+}
+
 __device__ __noinline__ void gemm(Ctx& c, CMat A, CMat B, OMat C, int M, int N, int K,
                                   double alpha, double beta) {
   if (M <= 0 || N <= 0) return;
   c.flops += 2.0 * M * N * (double)K;
   const long long t0 = clock64();
-  cta_gemm_pipe(A, B, C, M, N, K, alpha, beta, c.ring);
+  const int tiles = ((M + GBM - 1) / GBM) * ((N + GBN - 1) / GBN);
+  // shared out only with every operand and the output in global memory (a
+  // worker's shared-memory address names its own shared memory)
+  if (c.csize > 1 && tiles >= 2 && !__isShared(C.p) && gemm_pipe_tiled(A, B, M, N, K)) {
+    if (threadIdx.x == 0) {
+      ClusterCmd& q = *c.cmd;
+      q.op = CL_GEMM;
+      q.a = A.p;
+      q.a_rs = A.rs;
+      q.a_cs = A.cs;
+      q.b = B.p;
+      q.b_rs = B.rs;
+      q.b_cs = B.cs;
+      cmd_set_out(q, C);
+      q.M = M;
+      q.N = N;
+      q.K = K;
+      q.alpha = alpha;
+      q.beta = beta;
+    }
+    cluster_barrier();  // posted
+    cta_gemm_pipe(A, B, C, M, N, K, alpha, beta, c.ring, 0, c.csize);
+    cluster_barrier();  // every block's tiles are written
+  } else {
+    cta_gemm_pipe(A, B, C, M, N, K, alpha, beta, c.ring);
+  }
   c.cyc[PH_GEMM] += clock64() - t0;
 }
 
@@ -250,10 +448,55 @@ __device__ __noinline__ SpOp build_spop(Ctx& c, const double* op, int R, int n, 
 // OMat.  Warps take rows, lanes take columns; each element sums its row's
 // nonzero terms in column order, so the result does not depend on the
 // schedule.  beta == 0 never reads C.
+// The rows rank, rank + csize, ... of the product below (each row as the
+// whole product computes it).
+__device__ __noinline__ void spmm_rows(const int* ptr, const int* col, const double* val,
+                                       int rows, const double* B, i64 b_rs, i64 b_cs, OMat C,
+                                       int N, double alpha, double beta, int rank, int csize) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r = rank + csize * warp; r < rows; r += csize * TTB_WARPS) {
+    const int e0 = ptr[r], e1 = ptr[r + 1];
+    double* crow = C.p + C.row(r);
+    for (int j = lane; j < N; j += 32) {
+      const double* bj = B + (i64)j * b_cs;
+      double acc = 0.0;
+      for (int e = e0; e < e1; ++e) acc = fma(val[e], bj[(i64)col[e] * b_rs], acc);
+      double* cp = crow + C.col(j);
+      double v = alpha * acc;
+      if (beta != 0.0) v = fma(beta, *cp, v);
+      *cp = v;
+    }
+  }
+  __syncthreads();
+}
+
 __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_rs, i64 b_cs,
                                   OMat C, int N, double alpha, double beta) {
   c.flops += 2.0 * S.nnz * (double)N;
   const long long t0 = clock64();
+  if (c.csize > 1 && S.rows >= 2 * TTB_WARPS && !__isShared(C.p) && !__isShared(B) &&
+      !__isShared(S.val)) {
+    if (threadIdx.x == 0) {
+      ClusterCmd& q = *c.cmd;
+      q.op = CL_SPMM;
+      q.sp_ptr = S.ptr;
+      q.sp_col = S.col;
+      q.sp_val = S.val;
+      q.sp_rows = S.rows;
+      q.b = B;
+      q.b_rs = b_rs;
+      q.b_cs = b_cs;
+      cmd_set_out(q, C);
+      q.N = N;
+      q.alpha = alpha;
+      q.beta = beta;
+    }
+    cluster_barrier();
+    spmm_rows(S.ptr, S.col, S.val, S.rows, B, b_rs, b_cs, C, N, alpha, beta, 0, c.csize);
+    cluster_barrier();
+    c.cyc[PH_GEMM] += clock64() - t0;
+    return;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int r = warp; r < S.rows; r += TTB_WARPS) {
     const int e0 = S.ptr[r], e1 = S.ptr[r + 1];
@@ -270,6 +513,35 @@ __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_
   }
   __syncthreads();
   c.cyc[PH_GEMM] += clock64() - t0;
+}
+
+// A chunked vector pass (see vpass_chunk); returns the sum, the same on
+// every thread.  In a cluster the chunks are shared out and the leader
+// reads the other blocks' chunk sums over distributed shared memory.
+__device__ __noinline__ double vpass(Ctx& c, const VecArgs& q) {
+  double* red = c.sm->red;
+  if (c.csize <= 1) {
+    double sum = 0.0;
+    for (int k = 0; k < kVecChunks; ++k) sum += vpass_chunk(q, k, red);
+    return sum;
+  }
+  if (threadIdx.x == 0) {
+    c.cmd->op = CL_VEC;
+    c.cmd->vec = q;
+  }
+  cluster_barrier();  // posted
+  for (int k = 0; k < kVecChunks; k += c.csize) {
+    const double v = vpass_chunk(q, k, red);
+    if (threadIdx.x == 0) c.vpart[k] = v;
+  }
+  cluster_barrier();  // every chunk sum is written
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  double sum = 0.0;
+  for (int k = 0; k < kVecChunks; ++k) {
+    const double* part = cl.map_shared_rank(c.vpart, k % c.csize);
+    sum += part[k];
+  }
+  return sum;
 }
 
 // ---------------------------------------------------------------------------
@@ -691,10 +963,14 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   __syncthreads();
   // the odd last element goes to thread 0, after its pairs
   const bool tail = odd && threadIdx.x == 0;
+  // long vectors: the chunked passes a cluster shares out (vpass)
+  const bool chunked = N >= kVecChunkMin;
   int istop = 0;
   for (int itn = 1; itn <= maxit; ++itn) {
     const double s = 1.0 / beta;
-    {
+    if (chunked) {
+      vpass(c, VecArgs{VP_SCALE, 0, s, 0.0, 0.0, 0.0, v, r2, nullptr, nullptr, N});
+    } else {
       const double2* R2 = reinterpret_cast<const double2*>(r2);
       double2* V = reinterpret_cast<double2*>(v);
 #pragma unroll 4
@@ -708,8 +984,11 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     apply(c, L, v, y, 1, 1.0, 0.0, tc);
     if (c.status) return;
     // y -= (beta / oldb) r1 and alfa = v . y in one pass
-    double dot = 0.0;
-    {
+    double dot = 0.0, alfa;
+    if (chunked) {
+      alfa = vpass(c, VecArgs{VP_LANCZOS, itn == 1, itn >= 2 ? beta / oldb : 0.0, 0.0, 0.0, 0.0,
+                              y, r1, v, nullptr, N});
+    } else {
       const double f = itn >= 2 ? beta / oldb : 0.0;
       const double2* V = reinterpret_cast<const double2*>(v);
       const double2* R1 = reinterpret_cast<const double2*>(r1);
@@ -735,11 +1014,13 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
         }
         dot = fma(v[N - 1], yi, dot);
       }
+      alfa = block_sum(dot, red);
     }
-    const double alfa = block_sum(dot, red);
     const double g = alfa / beta;
-    double part = 0.0;
-    {
+    double part = 0.0, psum;
+    if (chunked) {
+      psum = vpass(c, VecArgs{VP_RESID, 0, g, 0.0, 0.0, 0.0, r1, y, r2, nullptr, N});
+    } else {
       const double2* Y = reinterpret_cast<const double2*>(y);
       const double2* R2 = reinterpret_cast<const double2*>(r2);
       double2* R1 = reinterpret_cast<double2*>(r1);
@@ -756,6 +1037,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
         r1[N - 1] = yi;
         part = fma(yi, yi, part);
       }
+      psum = block_sum(part, red);
     }
     {
       double* t = r1;
@@ -763,7 +1045,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
       r2 = t;
     }
     oldb = beta;
-    beta = sqrt(block_sum(part, red));
+    beta = sqrt(psum);
     tnorm2 += alfa * alfa + oldb * oldb + beta * beta;
     if (itn == 1 && beta / beta1 <= 10.0 * kEps) istop = -1;
     const double oldeps = epsln;
@@ -778,8 +1060,10 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     const double phi = cs * phibar;
     phibar = sn * phibar;
     const double denom = 1.0 / gamma;
-    double xs = 0.0;
-    {
+    double xs = 0.0, xsum;
+    if (chunked) {
+      xsum = vpass(c, VecArgs{VP_UPDATE, 0, oldeps, delta, denom, phi, w2, w, v, x, N});
+    } else {
       const double2* V = reinterpret_cast<const double2*>(v);
       const double2* W = reinterpret_cast<const double2*>(w);
       double2* W2 = reinterpret_cast<double2*>(w2);
@@ -804,6 +1088,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
         x[N - 1] = xi;
         xs = fma(xi, xi, xs);
       }
+      xsum = block_sum(xs, red);
     }
     {
       double* t = w2;
@@ -816,7 +1101,7 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     rhs1 = rhs2 - delta * z;
     rhs2 = -epsln * z;
     const double Anorm = sqrt(tnorm2);
-    const double ynorm = sqrt(block_sum(xs, red));
+    const double ynorm = sqrt(xsum);
     const double epsx = Anorm * ynorm * kEps;
     const double rnorm = phibar;
     const double test1 = (ynorm == 0.0 || Anorm == 0.0) ? INFINITY : rnorm / (Anorm * ynorm);
@@ -2028,19 +2313,14 @@ __device__ __noinline__ void amen_run(Ctx& c, int rmax) {
 // which the factorisations use only outside the mixed-precision solves.
 static_assert(TC_RING_BYTES <= kPoolBytes, "tensor-core stages must fit the pool");
 
-__global__ void __launch_bounds__(TTB_THREADS, 1)
-    k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
-  extern __shared__ __align__(16) double dyn[];
-  __shared__ Sm sm;
-  double* pool = dyn + GSTAGES * GSTAGE_D;
-  const ttb_amen_task_t* T = tasks + blockIdx.x;
-  Ctx c;
+// Per-block context of a task (both kernels).
+__device__ void init_ctx(Ctx& c, const ttb_amen_task_t* T, Sm* sm, double* dyn, int rmax) {
   c.T = T;
-  c.sm = &sm;
+  c.sm = sm;
   c.slab = T->slab;
   c.cap = T->slab_doubles;
   c.top = 0;
-  c.pool = pool;
+  c.pool = dyn + GSTAGES * GSTAGE_D;
   c.ring = dyn;
   c.gsm = reinterpret_cast<GemmSmem*>(dyn);
   c.d = T->d;
@@ -2056,8 +2336,17 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
   c.mixed = (T->precision == 1);
   c.flops_tc = 0.0;
   c.refine = 0;
+  c.csize = 1;
+  c.cmd = nullptr;
+  c.vpart = nullptr;
+}
+
+// The solve of task T by this block (the lone block or a cluster's leader),
+// with the tensor-core pipeline around it in mixed precision.
+__device__ void lead_solve(Ctx& c, Sm& sm, int rmax) {
+  const ttb_amen_task_t* T = c.T;
   if (c.mixed) {
-    c.tc.ring = reinterpret_cast<float*>(pool);
+    c.tc.ring = reinterpret_cast<float*>(c.pool);
     c.tc.mbar = sm.mbar;
     c.tc.slot = &sm.tmem_slot;
     tc_init(c.tc);
@@ -2069,6 +2358,67 @@ __global__ void __launch_bounds__(TTB_THREADS, 1)
       T->residuals[2 * T->max_sweeps + 14] = c.flops_tc;
       T->residuals[2 * T->max_sweeps + 15] = (double)c.refine;
     }
+  }
+}
+
+__global__ void __launch_bounds__(TTB_THREADS, 1)
+    k_amen(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
+  extern __shared__ __align__(16) double dyn[];
+  __shared__ Sm sm;
+  Ctx c;
+  init_ctx(c, tasks + blockIdx.x, &sm, dyn, rmax);
+  lead_solve(c, sm, rmax);
+}
+
+// A cluster's worker block: run the leader's commands until the exit one.
+// ``lead`` is the leader's command slot (distributed shared memory).
+__device__ __noinline__ void cluster_worker(Ctx& c, const ClusterCmd* lead, int rank) {
+  for (;;) {
+    cluster_barrier();  // a command is posted
+    ClusterCmd q = *lead;
+    if (q.op == CL_EXIT) {
+      cluster_barrier();  // the leader's shared memory stays until every block has read
+      return;
+    }
+    if (q.op == CL_GEMM) {
+      cta_gemm_pipe(CMat{q.a, q.a_rs, q.a_cs}, CMat{q.b, q.b_rs, q.b_cs}, cmd_out(q), q.M, q.N,
+                    q.K, q.alpha, q.beta, c.ring, rank, c.csize);
+    } else if (q.op == CL_VEC) {
+      for (int k = rank; k < kVecChunks; k += c.csize) {
+        const double v = vpass_chunk(q.vec, k, c.sm->red);
+        if (threadIdx.x == 0) c.vpart[k] = v;
+      }
+    } else {
+      spmm_rows(q.sp_ptr, q.sp_col, q.sp_val, q.sp_rows, q.b, q.b_rs, q.b_cs, cmd_out(q), q.N,
+                q.alpha, q.beta, rank, c.csize);
+    }
+    cluster_barrier();  // this block's share is written
+  }
+}
+
+// One solve per cluster of blocks (launched with a cluster dimension): the
+// leader (rank 0) runs it, the other blocks take shares of its products.
+__global__ void __launch_bounds__(TTB_THREADS, 1)
+    k_amen_cl(const ttb_amen_task_t* __restrict__ tasks, int rmax) {
+  extern __shared__ __align__(16) double dyn[];
+  __shared__ Sm sm;
+  __shared__ ClusterCmd cmd;
+  __shared__ double vpart[kVecChunks];
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int csize = (int)cl.num_blocks();
+  Ctx c;
+  init_ctx(c, tasks + blockIdx.x / csize, &sm, dyn, rmax);
+  c.csize = csize;
+  c.cmd = &cmd;
+  c.vpart = vpart;
+  if (rank == 0) {
+    lead_solve(c, sm, rmax);
+    if (threadIdx.x == 0) cmd.op = CL_EXIT;
+    cluster_barrier();
+    cluster_barrier();
+  } else {
+    cluster_worker(c, cl.map_shared_rank(&cmd, 0), rank);
   }
 }
 
@@ -2121,6 +2471,32 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   const long long step = 3 * N + K * n * K +
                          std::max({env, direct, iter, rank + fact, resid, 2 * rbmax * n * r});
   return slots + 2 * step + (1 << 16);
+}
+
+int ttb_amen_persistent_cluster(const ttb_amen_task_t* tasks, int count, int rmax, int cluster,
+                                void* stream) {
+  if (cluster <= 1) return ttb_amen_persistent(tasks, count, rmax, stream);
+  if (count <= 0) return 0;
+  if (cluster > 8) return (int)cudaErrorInvalidValue;
+  static int configured[kMaxDevices];
+  const size_t smem = kRingBytes + kPoolBytes;
+  if (int e = smem_limit_once((const void*)k_amen_cl, (int)smem, configured)) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(count * cluster), 1, 1);
+  cfg.blockDim = dim3(TTB_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = reinterpret_cast<cudaStream_t>(stream);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_amen_cl, tasks, rmax);
+  ttb::count_launch();
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaGetLastError();
 }
 
 int ttb_amen_persistent(const ttb_amen_task_t* tasks, int count, int rmax, void* stream) {

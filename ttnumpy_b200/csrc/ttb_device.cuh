@@ -361,8 +361,22 @@ static __device__ __noinline__ void cta_gemm_skinny(CMat A, CMat B, OMat C, int 
 constexpr int kSkinnyK = 128;
 static_assert(TTB_WARPS * 16 * 48 <= GSTAGES * GSTAGE_D, "split-K scratch must fit the ring");
 
+// True when cta_gemm_pipe takes its tiled path for these operands (not the
+// one-stage tile or the split-K product), the path whose output tiles may be
+// shared out between the blocks of a cluster (tile0, tstride below).
+static __device__ __forceinline__ bool gemm_pipe_tiled(CMat A, CMat B, int M, int N, int K) {
+  if (M <= 0 || N <= 0 || K <= 0 || __isShared(A.p) || __isShared(B.p)) return false;
+  if (K >= kSkinnyK && A.cs == 1 && B.rs == 1 && ((M <= 16 && N <= 48) || (M <= 48 && N <= 16)))
+    return false;
+  return true;
+}
+
+// ``tile0`` and ``tstride``: on the tiled path, compute only the output
+// tiles tile0, tile0 + tstride, ... (row-major tile order), each exactly as
+// the whole product computes it.
 static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
-                                                  double alpha, double beta, double* ring) {
+                                                  double alpha, double beta, double* ring,
+                                                  int tile0 = 0, int tstride = 1) {
   if (M <= 0 || N <= 0) return;
   // cp.async copies from global memory only: operands in shared memory, and
   // K == 0 (C = beta * C), go through the one-stage tile
@@ -387,12 +401,14 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
   const int g = lane >> 2, t = lane & 3;
   const int tn = (N + GBN - 1) / GBN;
   const int nk = (K + GBK - 1) / GBK;
-  const int total = ((M + GBM - 1) / GBM) * tn * nk;
+  const int tiles = ((M + GBM - 1) / GBM) * tn;
+  const int nloc = tile0 < tiles ? (tiles - tile0 + tstride - 1) / tstride : 0;
+  const int total = nloc * nk;
   const bool a_kfast = (A.cs == 1);
   const bool b_nfast = (B.cs == 1) || (B.rs != 1);
   auto issue = [&](int step) {
     if (step < total) {
-      const int tile = step / nk, kt = step % nk;
+      const int tile = tile0 + (step / nk) * tstride, kt = step % nk;
       const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN, k0 = kt * GBK;
       double* sa = ring + (step % GSTAGES) * GSTAGE_D;
       double* sb = sa + GBK * GPITCH_A;
@@ -447,7 +463,7 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
         for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
     }
     if (kt == nk - 1) {
-      const int tile = step / nk;
+      const int tile = tile0 + (step / nk) * tstride;
       const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN;
       i64 coff[2][2];
 #pragma unroll

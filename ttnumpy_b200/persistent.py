@@ -184,9 +184,10 @@ class PersistentBatch:
     """
 
     def __init__(self, preps: List["_Prepared"], rmax: int, debug: bool = False,
-                 time_limit: Optional[float] = None, resident: bool = False):
+                 time_limit: Optional[float] = None, resident: bool = False, cluster: int = 1):
         lib = _lib_handle()
         self.preps, self.rmax = preps, rmax
+        self.cluster = max(1, int(cluster))  # thread blocks per solve
         n = len(preps)
         # inputs: per request already on the device (``resident``: uploaded
         # beforehand by _Prepared.resident), or packed here into one buffer
@@ -268,6 +269,11 @@ class PersistentBatch:
     def launch(self, stream: Optional[torch.cuda.Stream] = None) -> None:
         """Queue the kernel on ``stream`` (asynchronous)."""
         s = stream or torch.cuda.current_stream()
+        if self.cluster > 1:
+            check(K.lib().ttb_amen_persistent_cluster(
+                C.c_void_p(self.dev_tasks.data_ptr()), len(self.preps), self.rmax, self.cluster,
+                C.c_void_p(s.cuda_stream)), "ttb_amen_persistent_cluster")
+            return
         check(K.lib().ttb_amen_persistent(C.c_void_p(self.dev_tasks.data_ptr()),
                                           len(self.preps), self.rmax, C.c_void_p(s.cuda_stream)),
               "ttb_amen_persistent")
@@ -380,6 +386,13 @@ def initial_rmax(p: "_Prepared") -> int:
     return 64 if n < 64 else 96
 
 
+def cluster_size(p: "_Prepared") -> int:
+    """Thread blocks a request's solve runs on: four for mode sizes of 64
+    and up, whose local operator applications are the large products a
+    cluster shares out (tens of seconds of work on one SM), one otherwise."""
+    return 4 if max(p.modes) >= 64 else 1
+
+
 def _cost(p: "_Prepared") -> float:
     """Relative cost estimate of a solve for the launch order: the local
     apply grows like n^3 R^2 at the bonds such problems reach, times d."""
@@ -395,18 +408,19 @@ def prepare(requests: Sequence) -> List["_Prepared"]:
 
 def amen_persistent(requests: Sequence, rmax: int = 64, max_rmax: int = 256,
                     stream: Optional[torch.cuda.Stream] = None,
-                    time_limit: Optional[float] = None) -> List[Result]:
+                    time_limit: Optional[float] = None, cluster: int = 1) -> List[Result]:
     """Solve ``[(A, b, x0, kwargs), ...]`` in one persistent launch; solves
     whose bonds outgrow ``rmax`` are re-run with twice the capacity.  With
     ``time_limit`` (seconds) a solve still running after that long on the
-    device stops with status -6."""
+    device stops with status -6; with ``cluster`` > 1 every solve runs on a
+    cluster of that many thread blocks (same results)."""
     K.device_ok()
     preps = prepare(requests)
     results: List[Optional[Result]] = [None] * len(preps)
     todo = list(range(len(preps)))
     while todo:
-        out = PersistentBatch([preps[i] for i in todo], rmax,
-                              time_limit=time_limit).run(stream)
+        out = PersistentBatch([preps[i] for i in todo], rmax, time_limit=time_limit,
+                              cluster=cluster).run(stream)
         retry = []
         for i, res in zip(todo, out):
             if res.status == -4 and rmax < max_rmax:

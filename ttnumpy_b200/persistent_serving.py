@@ -12,8 +12,10 @@ are read back when its completion event has fired.
 
 Each request starts at a slot capacity chosen from its mode sizes
 (``initial_rmax``); one whose bonds outgrow it (status -4) is queued again
-with twice the capacity, as ``amen_persistent`` does.  A launch takes
-requests of one capacity, that of the oldest waiting request.
+with twice the capacity, as ``amen_persistent`` does.  Requests with mode
+sizes of 64 and up run on clusters of four thread blocks (``cluster_size``),
+the others on one.  A launch takes requests of one capacity and cluster
+size, those of the oldest waiting request.
 
 Requests are admitted by device memory: with ``mem_budget`` set, a launch
 takes waiting requests only while the work areas (slabs) of all launches in
@@ -33,7 +35,8 @@ from typing import Callable, List, Optional, Sequence
 import torch
 
 from . import kernels as K
-from .persistent import PersistentBatch, Result, _cost, _Prepared, initial_rmax, slab_doubles
+from .persistent import (PersistentBatch, Result, _cost, _Prepared, cluster_size, initial_rmax,
+                         slab_doubles)
 
 
 def admit(sizes: Sequence[int], room: Optional[int], idle: bool) -> List[int]:
@@ -64,6 +67,7 @@ class Job:
     arrival: float
     prep: _Prepared
     rmax: int
+    cluster: int = 1  # thread blocks of its solve
     result: Optional[Result] = None
     slab_bytes: int = 0  # work area at the current slot capacity
     done_at: Optional[float] = None
@@ -85,7 +89,8 @@ class PersistentServer:
 
     def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: Optional[int] = None,
                  max_rmax: int = 256, min_interval: float = 0.005, download: bool = True,
-                 mem_budget: Optional[int] = None, resident: bool = False):
+                 mem_budget: Optional[int] = None, resident: bool = False,
+                 cluster_for: Optional[Callable[[_Prepared], int]] = cluster_size):
         K.device_ok()
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.free = list(range(streams))
@@ -96,6 +101,7 @@ class PersistentServer:
         self.download = download
         self.mem_budget = mem_budget
         self.resident = resident  # inputs uploaded before submission (no copy per launch)
+        self.cluster_for = cluster_for  # thread blocks per solve (None: one)
         self.inflight_bytes = 0
         self.peak_bytes = 0
         self.queue: List[Job] = []
@@ -113,7 +119,8 @@ class PersistentServer:
     def submit_prepared(self, rid: int, arrival: float, prep: _Prepared) -> Job:
         """Queue an already validated request; it starts at the server's
         slot capacity, or at ``initial_rmax`` for its mode sizes."""
-        job = Job(rid, arrival, prep, self.rmax or initial_rmax(prep))
+        job = Job(rid, arrival, prep, self.rmax or initial_rmax(prep),
+                  self.cluster_for(prep) if self.cluster_for else 1)
         job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
         self.queue.append(job)
         return job
@@ -125,8 +132,8 @@ class PersistentServer:
             return False
         # one slot capacity per launch: the oldest waiting request's, so that
         # requests of every capacity are launched in arrival order
-        rmax = self.queue[0].rmax
-        take = [j for j in self.queue if j.rmax == rmax][: self.max_batch]
+        rmax, cl = self.queue[0].rmax, self.queue[0].cluster
+        take = [j for j in self.queue if j.rmax == rmax and j.cluster == cl][: self.max_batch]
         room = None if self.mem_budget is None else self.mem_budget - self.inflight_bytes
         idx = admit([j.slab_bytes for j in take], room, not self.inflight)
         if not idx:
@@ -138,7 +145,8 @@ class PersistentServer:
         si = self.free.pop()
         s = self.streams[si]
         with torch.cuda.stream(s):
-            batch = PersistentBatch([j.prep for j in take], rmax, resident=self.resident)
+            batch = PersistentBatch([j.prep for j in take], rmax, resident=self.resident,
+                                    cluster=cl)
             batch.launch(s)
             ev = torch.cuda.Event()
             ev.record(s)
