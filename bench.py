@@ -78,12 +78,20 @@ def parse(argv=None):
     ap.add_argument("--max-batch", type=int, default=8, help="requests per server launch")
     ap.add_argument("--plain-sample", type=int, default=64,
                     help="requests timed through the plain one-at-a-time drop-in (0: skip)")
-    ap.add_argument("--plain-limit", type=float, default=2.0,
-                    help="per-solve time limit (s) of the plain drop-in sample")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="requests in the CPU baseline sample (0: two per host core)")
-    ap.add_argument("--cpu-limit", type=float, default=30.0,
-                    help="per-solve time limit (s) of the CPU oracle solves")
+    ap.add_argument("--plain-limit", type=float, default=2.0,
+                    help="per-solve time limit (s) of the plain drop-in sample (shorter than "
+                         "--time-limit, which can only favour the plain baseline)")
+    ap.add_argument("--time-limit", type=float, default=30.0,
+                    help="per-solve time limit (s), the same for every arm: device time of a "
+                         "solve on the GPU, host time on the CPU; a solve stopped by it counts "
+                         "as not solved")
+    ap.add_argument("--cluster", action="store_true",
+                    help="run mode-64 requests on clusters of four thread blocks")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="only run the small profiling case (one persistent launch of 8 "
+                         "requests, twice) and print its per-request device times")
     return ap.parse_args(argv)
 
 
@@ -311,9 +319,12 @@ def _solved(job) -> bool:
 def make_server(args, resident: bool, download: bool):
     from ttnumpy_b200.persistent_serving import PersistentServer
 
+    from ttnumpy_b200.persistent import cluster_size
+
     return PersistentServer(streams=args.streams, max_batch=args.max_batch,
                             mem_budget=int(args.serve_mem_gb * 2**30), resident=resident,
-                            download=download)
+                            download=download, time_limit=args.time_limit,
+                            cluster_for=cluster_size if args.cluster else None)
 
 
 def resident_run(args, preps, torch):
@@ -422,6 +433,14 @@ def config1_run(torch):
     out["persistent_device_s"] = r.device_ms * 1e-3
     out["persistent"] = {"status": r.status, "sweeps": r.info.num_sweeps_run,
                          "residual": r.info.residuals[-1] if r.info.residuals else None}
+    for cl in (4, 8):  # the same solve on a cluster of blocks (same bits, shorter wall time)
+        t0 = time.perf_counter()
+        rc = amen_persistent([(p.A, p.b, None, kw)], rmax=64, cluster=cl)[0]
+        torch.cuda.synchronize()
+        out[f"cluster{cl}_s"] = time.perf_counter() - t0
+        out[f"cluster{cl}_same_bits"] = bool(
+            rc.status == 0 and rc.info.residuals == r.info.residuals
+            and all(np.array_equal(u, v) for u, v in zip(rc.x.to_numpy(), r.x.to_numpy())))
     t0 = time.perf_counter()
     x, info = tt.amen(tt.TensorTrain(p.A), tt.TensorTrain(p.b), return_info=True, **kw)
     torch.cuda.synchronize()
@@ -468,8 +487,42 @@ def rounding_run(torch, pairs=1024, reps=5):
             "precision": "float64 (no 3xTF32 rounding variant)"}
 
 
+def profile_case():
+    """The small case profiled with ncu: one persistent launch of 8 requests
+    (2-D QTT Poisson with 8, 12, 16, 20 cores; diffusion d = 4, 6 with
+    n = 16, 32), run twice (the second launch is the captured one)."""
+    import torch
+
+    from ttnumpy_b200 import problems as P
+    from ttnumpy_b200.persistent import PersistentBatch, prepare
+
+    torch.cuda.set_device(0)
+    kw = dict(residual_tol=TOL, symmetric=True, max_sweeps=MAX_SWEEPS, seed=0,
+              stagnation_factor=None)
+    rng = np.random.default_rng(11)
+    reqs = []
+    for N in (4, 6, 8, 10):
+        p = P.qtt_poisson_2d(N)
+        p.meta["kind"] = "qtt"
+        reqs.append((p.A, p.b, x0_host(p), kw))
+    for d, n in ((4, 16), (4, 32), (6, 16), (6, 32)):
+        q = P.parametric_diffusion(d, n, rng.uniform(-1, 1, size=d))
+        reqs.append((q.A, q.b, None, kw))
+    batch = PersistentBatch(prepare(reqs), 64)
+    for _ in range(2):
+        batch.launch()
+        torch.cuda.synchronize()
+    res = batch.collect()
+    print(json.dumps({"status": [r.status for r in res],
+                      "gflop": sum(r.flops for r in res) / 1e9,
+                      "device_ms": [round(r.device_ms, 1) for r in res]}))
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case()
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -579,7 +632,7 @@ def main():
     cpu = None
     if world == 1:
         n_cpu = args.cpu_sample or 2 * cpu_cores()
-        cpu = cpu_baseline(reqs[:n_cpu], cpu_cores(), args.cpu_limit)
+        cpu = cpu_baseline(reqs[:n_cpu], cpu_cores(), args.time_limit)
         # config 1 on one host core, uncapped (the secondary single-solve line)
         dt, conv, _ = cpu_run([config1_problem()], 1, 1e9)[1][0]
         secondary["config1_single_solve"]["cpu_oracle_s"] = dt
@@ -609,12 +662,12 @@ def reference_main(args):
     reqs = make_requests((args.warmup + args.steps) * B, args.seed, args.preset)
     small = [p for p in reqs if p.meta["kind"] == "qtt"][:cores] or reqs[:1]
     for _ in range(args.warmup):
-        cpu_run(small, cores, args.cpu_limit)
+        cpu_run(small, cores, args.time_limit)
     total, cpu_s, res_all = 0.0, 0.0, []
     for k in range(args.steps):
         start = (args.warmup + k) * B
         sample = reqs[start:start + min(cores, B)]
-        dt, res = cpu_run(sample, cores, args.cpu_limit)
+        dt, res = cpu_run(sample, cores, args.time_limit)
         total += dt
         cpu_s += sum(r[0] for r in res)
         res_all += res
@@ -623,7 +676,7 @@ def reference_main(args):
     sample_txt = (f"{min(cores, B)} requests per step (the first of each step's batch of the "
                   "stream), "
                   f"{cores} single-threaded oracle workers, each solve capped at "
-                  f"{args.cpu_limit:g} s; value = solved / (sum of solve seconds / cores)")
+                  f"{args.time_limit:g} s; value = solved / (sum of solve seconds / cores)")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
@@ -655,7 +708,12 @@ def config(args, engine="persistent server"):
                 "(d in 4,5, n in 16,32); residual 1e-8, at most 30 sweeps")
     out = {"workload": work, "requests_per_step": args.requests, "engine": engine,
            "max_sweeps": MAX_SWEEPS, "stagnation_factor": None,
+           "per_solve_time_limit_s": args.time_limit,
+           "time_limit_rule": "the same in every arm (device time of a solve on the GPU, host "
+                              "time of a solve on the CPU); a solve stopped by it is not solved",
            "parallelism": f"replicas x{args.gpus}"}
+    if engine != "reference":
+        out["cluster"] = "mode-64 requests on clusters of 4 blocks" if args.cluster else "one block per solve"
     if engine != "reference":
         out["l2"] = ("inputs larger than L2 (each request's work area is tens to hundreds of "
                      "MB); 512 MB flush before the timed region")

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_json_line():
     cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
            "--preset", "small", "--requests", "4", "--steps", "1", "--warmup", "0",
-           "--cpu-limit", "10"]
+           "--time-limit", "10"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True).stdout
     lines = [ln for ln in out.splitlines() if ln.startswith("{")]
     assert len(lines) == 1

@@ -785,7 +785,7 @@ __device__ __noinline__ void qr(Ctx& c, CMat A, int m, int k, Mat Q, Mat R) {
   if (!Q.p && p > LNB2 && m >= 4 * k) {
     // R only of a tall matrix (the residual norm sweep): two-level blocking
     cta_qr_r_blocked2(A, m, k, W, W + (i64)m * k, R, c.pool, c.sm->red, c.ring);
-    if (c.T->debug) {
+    if (c.T->debug & 1) {
       // the one-level blocked factorisation of the same matrix, compared
       double* R1 = take(c, (i64)p * k);
       if (c.status) return;
@@ -1511,7 +1511,7 @@ __device__ __noinline__ int choose_rank(Ctx& c, int k, const double* u, const do
   __syncthreads();
   int rank = limit;
   const bool forward = (M == L.lt * L.m);
-  if (T->debug) {
+  if (T->debug & 1) {
     // one term at a time, each also applied in full for the self-check
     double* term = take(c, N);
     if (c.status) return 1;

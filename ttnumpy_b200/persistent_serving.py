@@ -90,7 +90,8 @@ class PersistentServer:
     def __init__(self, streams: int = 16, max_batch: int = 1024, rmax: Optional[int] = None,
                  max_rmax: int = 256, min_interval: float = 0.005, download: bool = True,
                  mem_budget: Optional[int] = None, resident: bool = False,
-                 cluster_for: Optional[Callable[[_Prepared], int]] = cluster_size):
+                 cluster_for: Optional[Callable[[_Prepared], int]] = cluster_size,
+                 time_limit: Optional[float] = None):
         K.device_ok()
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.free = list(range(streams))
@@ -102,6 +103,7 @@ class PersistentServer:
         self.mem_budget = mem_budget
         self.resident = resident  # inputs uploaded before submission (no copy per launch)
         self.cluster_for = cluster_for  # thread blocks per solve (None: one)
+        self.time_limit = time_limit    # per-solve device-time limit (s), status -6 past it
         self.inflight_bytes = 0
         self.peak_bytes = 0
         self.queue: List[Job] = []
@@ -146,7 +148,7 @@ class PersistentServer:
         s = self.streams[si]
         with torch.cuda.stream(s):
             batch = PersistentBatch([j.prep for j in take], rmax, resident=self.resident,
-                                    cluster=cl)
+                                    cluster=cl, time_limit=self.time_limit)
             batch.launch(s)
             ev = torch.cuda.Event()
             ev.record(s)
