@@ -2131,6 +2131,8 @@ __device__ __noinline__ void amen_run(Ctx& c, int rmax) {
     if (threadIdx.x == 0) {                                        \
       T->result[0] = c.status;                                     \
       T->result[1] = sweeps;                                       \
+      T->residuals[2 * T->max_sweeps] = c.flops;                   \
+      T->residuals[2 * T->max_sweeps + 1] = (double)c.applies;     \
       T->residuals[2 * T->max_sweeps + 10] = (double)t_start;      \
       T->residuals[2 * T->max_sweeps + 11] = (double)global_ns();  \
     }                                                              \
