@@ -66,7 +66,7 @@ def parse(argv=None):
     ap.add_argument("--requests", type=int, default=148,
                     help="requests per step (148 = one per SM of a B200)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--serve-requests", type=int, default=400,
+    ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests in each served pass (a slice of the stream after the "
                          "timed steps' requests)")
     ap.add_argument("--serve-loads", default="0.8",

@@ -150,6 +150,25 @@ def test_cluster_equals_lone_block(pers):
         assert all(np.array_equal(u, v) for u, v in zip(a.x.to_numpy(), b.x.to_numpy())), p.name
 
 
+def test_graph_replay_equals_launch(pers):
+    """The batch's launch captured in a CUDA graph and replayed re-solves
+    every request with the same bits, lone blocks and clusters alike."""
+    kw = dict(residual_tol=1e-8, symmetric=True, max_sweeps=8, seed=0, stagnation_factor=None)
+    probs = [_diffusion(12, 4, 32), P.qtt_poisson_2d(5)]
+    for cluster in (1, 2):
+        batch = pers.PersistentBatch(pers.prepare([(p.A, p.b, None, kw) for p in probs]), 64,
+                                     cluster=cluster)
+        first = batch.run()
+        graph = batch.capture()
+        graph.replay()
+        torch.cuda.synchronize()
+        again = batch.collect()
+        for a, b in zip(first, again):
+            assert a.status == 0 and b.status == 0
+            assert a.info.residuals == b.info.residuals
+            assert all(np.array_equal(u, v) for u, v in zip(a.x.to_numpy(), b.x.to_numpy()))
+
+
 def test_matches_dropin(pers):
     import ttnumpy_b200 as tt
 

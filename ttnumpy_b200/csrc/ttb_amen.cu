@@ -27,7 +27,8 @@ namespace {
 using namespace ttb;
 
 constexpr int kD = 64;                 // most cores per train
-constexpr int kPoolBytes = 160 * 1024;  // dynamic shared-memory pool (after the GEMM ring)
+// dynamic shared-memory pool (after the GEMM ring, whose size follows GBK)
+constexpr int kPoolBytes = (GBK == 16 ? 160 : 114) * 1024;
 constexpr int kRingBytes = GSTAGES * GSTAGE_D * 8;
 constexpr i64 kPoolD = kPoolBytes / 8;
 // fixed-size pool users: the two-level R-only QR's panel buffers and the
@@ -860,15 +861,13 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
   const i64 mark = c.top;
   Sm* s = c.sm;
   double* W;
+  double* panel = c.pool;  // the blocked elimination's panel (N x LNB)
   const bool small = N * N + N <= kPoolD;
   if (small) {
     W = c.pool;
   } else {
-    if (N * LNB > kPoolD) {
-      c.status = ST_SETTINGS;
-      return;
-    }
     W = take(c, N * N);
+    if (N * LNB > kPoolD) panel = take(c, N * LNB);  // beyond the pool: in the slab
     if (c.status) return;
   }
   // explicit local matrix, column major: each thread owns rows (j, kr, nf)
@@ -909,7 +908,7 @@ __device__ __noinline__ void direct_solve(Ctx& c, const LocalOp& L, const double
     __syncthreads();
     if (info == 0) vcopy(u, bb, N);
   } else {
-    info = cta_gepp_blocked(W, N, u, (int)N, c.pool, s->red, s->redi, s->ipiv, *c.gsm, c.ring);
+    info = cta_gepp_blocked(W, N, u, (int)N, panel, s->red, s->redi, s->ipiv, *c.gsm, c.ring);
   }
   __syncthreads();
   if (info != 0) c.status = ST_SINGULAR;
@@ -2459,7 +2458,7 @@ long long ttb_amen_slab_doubles(int d, const int* dims, int kickrank, int rmax,
   const long long env = 2 * r * R * n * r + r * n * r + sp;
   const long long apply = 2 * r * n * R * r + R * n * n * R + R * r * r + 2 * sp;  // + permute_op
   const long long dn = std::min<long long>(direct_solve_size, N);
-  const long long direct = dn * dn + dn;
+  const long long direct = dn * dn + dn + dn * LNB;
   // MINRES: six vectors; GMRES: restart + 3 vectors and the Hessenberg data
   const long long iter = N + std::max(6 * N, (kRestart + 3) * (N + 32) + 2048) + apply;
   const long long rank = 4 * N + 2LL * kRankChunk * R * n * r + R * r * r + r * r + apply;

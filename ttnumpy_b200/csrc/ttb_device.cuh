@@ -99,7 +99,11 @@ struct CMat {
 // ---------------------------------------------------------------------------
 
 // Tile rows: 32 per four warps (64 for 8 warps, 96 for 12), 64 columns.
-constexpr int GBM = 8 * TTB_WARPS, GBN = 64, GBK = 16;
+// K depth of a staged slab (16, or 32 for half the block barriers per K)
+#ifndef TTB_GBK
+#define TTB_GBK 16
+#endif
+constexpr int GBM = 8 * TTB_WARPS, GBN = 64, GBK = TTB_GBK;
 // Row pitches of the staged tiles: 4 more than a multiple of 16 doubles puts
 // the four k-rows a fragment load touches on disjoint bank groups, so each
 // load takes two wavefronts.

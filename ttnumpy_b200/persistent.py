@@ -278,6 +278,18 @@ class PersistentBatch:
                                           len(self.preps), self.rmax, C.c_void_p(s.cuda_stream)),
               "ttb_amen_persistent")
 
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """The batch's launch captured in a CUDA graph: ``graph.replay()``
+        solves every request of the batch again (the kernel only reads the
+        inputs, which may be updated in place between replays, and rewrites
+        every result), then :meth:`collect` reads the results.  Run the batch
+        once first, so that the one-time set-up of the library happens
+        outside the capture."""
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.launch()
+        return graph
+
     def gemm_flops(self) -> float:
         """FP64 FLOPs of the dense products of the last launch, all blocks."""
         resid_h = self.resid.cpu().numpy()
