@@ -72,3 +72,27 @@ def test_work_area_bounds(lib):
     assert all(v >= 0 for v in qr + svd)
     assert qr == sorted(qr) and svd == sorted(svd)
     assert lib.ttb_lu_work_doubles(2000) >= 2000
+
+
+def test_serving_mix_generator():
+    """The serving stream's requests: one seeded generator, the same
+    requests for the same seed, about 10 % large, the rest split between
+    diffusion and QTT Poisson, with the stated dimension and mode ranges."""
+    from ttnumpy_b200 import problems as P
+
+    a = P.serving_requests(400, 3)
+    b = P.serving_requests(400, 3)
+    assert [p.name for p in a] == [p.name for p in b]
+    assert all(np.array_equal(x, y) for p, q in zip(a, b) for x, y in zip(p.A, q.A))
+    kinds = [p.meta["kind"] for p in a]
+    assert 20 <= kinds.count("large") <= 60
+    assert 140 <= kinds.count("diffusion") <= 220 and 140 <= kinds.count("qtt") <= 220
+    for p in a:
+        if p.meta["kind"] == "diffusion":
+            assert 4 <= len(p.A) <= 12 and p.A[0].shape[1] in (16, 32, 64)
+        elif p.meta["kind"] == "qtt":
+            assert len(p.A) % 2 == 0 and 6 <= len(p.A) <= 20
+        else:
+            assert len(p.A) == 24 and p.A[0].shape[1] == 64 and max(c.shape[0] for c in p.b) == 8
+    arrivals = [t for t, _ in P.serving_stream(50, rate=10.0, seed=3)]
+    assert all(t1 > t0 for t0, t1 in zip(arrivals, arrivals[1:]))
