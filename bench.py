@@ -76,6 +76,8 @@ def parse(argv=None):
                     help="device memory the server may hold in work areas of requests in flight")
     ap.add_argument("--streams", type=int, default=32, help="server launch streams")
     ap.add_argument("--max-batch", type=int, default=8, help="requests per server launch")
+    ap.add_argument("--light-streams", type=int, default=8,
+                    help="high-priority server streams for light requests (0: one lane)")
     ap.add_argument("--plain-sample", type=int, default=64,
                     help="requests timed through the plain one-at-a-time drop-in (0: skip)")
     ap.add_argument("--cpu-sample", type=int, default=0,
@@ -324,7 +326,8 @@ def make_server(args, resident: bool, download: bool):
     return PersistentServer(streams=args.streams, max_batch=args.max_batch,
                             mem_budget=int(args.serve_mem_gb * 2**30), resident=resident,
                             download=download, time_limit=args.time_limit,
-                            cluster_for=cluster_size if args.cluster else None)
+                            cluster_for=cluster_size if args.cluster else None,
+                            light_streams=args.light_streams)
 
 
 def resident_run(args, preps, torch):
@@ -599,7 +602,8 @@ def main():
            "d2h_bytes_per_step": int(sat["d2h"] * B / n_pass),
            "mode": f"served: {sat['requests']} requests of the stream from host memory arriving "
                    f"as a Poisson stream at {sat['rate']:.2f}/s (twice the measured capacity), "
-                   f"continuous batching over {args.streams} streams of persistent launches of "
+                   f"continuous batching over {args.streams} streams (and {args.light_streams} "
+                   "high-priority streams for light requests) of persistent launches of "
                    f"at most {args.max_batch} requests admitted by a {args.serve_mem_gb:g} GB "
                    "work-area budget, inputs copied per launch, solutions read back; bytes per "
                    f"step scaled to {B} requests",

@@ -40,14 +40,23 @@ def _problems():
     return out
 
 
-def test_staggered_arrivals_match_alone(srv_mod):
+@pytest.mark.parametrize("light_streams", [0, 2])
+def test_staggered_arrivals_match_alone(srv_mod, light_streams):
+    """With light_streams, the QTT requests (the light ones) are served from
+    their own queue on high-priority streams; results are the same either
+    way."""
     pers, ps = srv_mod
     probs = _problems()
     reqs = [(p.A, p.b, None, KW) for p in probs]
     arrivals = [0.0, 0.0, 0.01, 0.02, 0.02, 0.05, 0.08, 0.08, 0.12, 0.2]
-    server = ps.PersistentServer(streams=4, min_interval=0.002)
+    server = ps.PersistentServer(streams=4, min_interval=0.002, light_streams=light_streams)
     jobs = server.serve(reqs, arrivals)
     assert server.launches >= 2
+    lanes = [j.lane for j in jobs]
+    if light_streams:
+        assert lanes == [0 if i % 2 == 0 else 1 for i in range(len(jobs))]
+    else:
+        assert set(lanes) == {1}
     for p, job in zip(probs, jobs):
         res = job.result
         assert res.status == 0 and res.info.converged, (p.name, res.info)

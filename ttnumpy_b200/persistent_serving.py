@@ -17,6 +17,11 @@ sizes of 64 and up run on clusters of four thread blocks (``cluster_size``),
 the others on one.  A launch takes requests of one capacity and cluster
 size, those of the oldest waiting request.
 
+With ``light_streams``, requests whose estimated cost is at most
+``light_cost`` (the 2-D QTT Poisson problems of the serving mix) wait in a
+queue of their own and launch on streams of the highest priority, so that a
+burst of long solves does not hold them back.
+
 Requests are admitted by device memory: with ``mem_budget`` set, a launch
 takes waiting requests only while the work areas (slabs) of all launches in
 flight stay within the budget, so a burst of arrivals queues on the host
@@ -68,6 +73,7 @@ class Job:
     prep: _Prepared
     rmax: int
     cluster: int = 1  # thread blocks of its solve
+    lane: int = 1     # 0: light requests (own queue, high-priority streams), 1: the rest
     result: Optional[Result] = None
     slab_bytes: int = 0  # work area at the current slot capacity
     done_at: Optional[float] = None
@@ -91,10 +97,21 @@ class PersistentServer:
                  max_rmax: int = 256, min_interval: float = 0.005, download: bool = True,
                  mem_budget: Optional[int] = None, resident: bool = False,
                  cluster_for: Optional[Callable[[_Prepared], int]] = cluster_size,
-                 time_limit: Optional[float] = None):
+                 time_limit: Optional[float] = None, light_streams: int = 0,
+                 light_cost: float = 1e5):
         K.device_ok()
-        self.streams = [torch.cuda.Stream() for _ in range(streams)]
-        self.free = list(range(streams))
+        # lane 1: ``streams`` streams of normal priority; lane 0 (with
+        # ``light_streams``): requests of estimated cost at most
+        # ``light_cost`` in their own queue, launched on streams of the
+        # highest priority, so the block scheduler gives them the next free
+        # SMs instead of leaving them behind long solves
+        # (a priority beyond the device's range maps to its highest)
+        self.streams = ([torch.cuda.Stream(priority=-10) for _ in range(light_streams)]
+                        + [torch.cuda.Stream() for _ in range(streams)])
+        self.lane_of = [0] * light_streams + [1] * streams
+        self.free = {0: list(range(light_streams)),
+                     1: list(range(light_streams, light_streams + streams))}
+        self.light_cost = light_cost if light_streams > 0 else -1.0
         self.max_batch = max_batch
         self.rmax = rmax
         self.max_rmax = max_rmax
@@ -106,13 +123,13 @@ class PersistentServer:
         self.time_limit = time_limit    # per-solve device-time limit (s), status -6 past it
         self.inflight_bytes = 0
         self.peak_bytes = 0
-        self.queue: List[Job] = []
+        self.queues = {0: [], 1: []}  # waiting requests per lane, oldest first
         self.inflight = []  # (stream index, batch, event, jobs, slab bytes)
         self.completed: List[Job] = []
         self.launches = 0
         self.h2d_bytes = 0
         self.d2h_bytes = 0
-        self._last_launch = -1e30
+        self._last_launch = {0: -1e30, 1: -1e30}
 
     def submit(self, rid: int, arrival: float, A, b, x0=None, kwargs: Optional[dict] = None) -> Job:
         """Validate a request on the host and queue it (``amen`` arguments)."""
@@ -122,29 +139,39 @@ class PersistentServer:
         """Queue an already validated request; it starts at the server's
         slot capacity, or at ``initial_rmax`` for its mode sizes."""
         job = Job(rid, arrival, prep, self.rmax or initial_rmax(prep),
-                  self.cluster_for(prep) if self.cluster_for else 1)
+                  self.cluster_for(prep) if self.cluster_for else 1,
+                  0 if _cost(prep) <= self.light_cost else 1)
         job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
-        self.queue.append(job)
+        self.queues[job.lane].append(job)
         return job
 
+    @property
+    def queue(self) -> List[Job]:
+        """Every waiting request (both lanes)."""
+        return self.queues[0] + self.queues[1]
+
     def _launch(self, now: float) -> bool:
-        if not self.queue or not self.free:
+        return any([self._launch_lane(lane, now) for lane in (0, 1)])
+
+    def _launch_lane(self, lane: int, now: float) -> bool:
+        queue, free = self.queues[lane], self.free[lane]
+        if not queue or not free:
             return False
-        if len(self.queue) < self.max_batch and now - self._last_launch < self.min_interval:
+        if len(queue) < self.max_batch and now - self._last_launch[lane] < self.min_interval:
             return False
         # one slot capacity per launch: the oldest waiting request's, so that
         # requests of every capacity are launched in arrival order
-        rmax, cl = self.queue[0].rmax, self.queue[0].cluster
-        take = [j for j in self.queue if j.rmax == rmax and j.cluster == cl][: self.max_batch]
+        rmax, cl = queue[0].rmax, queue[0].cluster
+        take = [j for j in queue if j.rmax == rmax and j.cluster == cl][: self.max_batch]
         room = None if self.mem_budget is None else self.mem_budget - self.inflight_bytes
         idx = admit([j.slab_bytes for j in take], room, not self.inflight)
         if not idx:
             return False
         take = [take[i] for i in idx]
         taken = set(id(j) for j in take)
-        self.queue = [j for j in self.queue if id(j) not in taken]
+        self.queues[lane] = [j for j in queue if id(j) not in taken]
         take.sort(key=lambda j: -_cost(j.prep))
-        si = self.free.pop()
+        si = free.pop()
         s = self.streams[si]
         with torch.cuda.stream(s):
             batch = PersistentBatch([j.prep for j in take], rmax, resident=self.resident,
@@ -158,7 +185,7 @@ class PersistentServer:
         self.peak_bytes = max(self.peak_bytes, self.inflight_bytes)
         self.inflight.append((si, batch, ev, take, nbytes))
         self.launches += 1
-        self._last_launch = now
+        self._last_launch[lane] = now
         return True
 
     def _collect(self, now: float) -> bool:
@@ -176,7 +203,7 @@ class PersistentServer:
                     if res.status == -4 and job.rmax < self.max_rmax:
                         job.rmax = min(2 * job.rmax, self.max_rmax)
                         job.slab_bytes = 8 * slab_doubles(job.prep, job.rmax)
-                        self.queue.append(job)
+                        self.queues[job.lane].append(job)
                         continue
                     job.result = res
                     if self.download and res.x is not None:
@@ -185,7 +212,7 @@ class PersistentServer:
                     job.done_at = now
                     self.completed.append(job)
             batch.release()
-            self.free.append(si)
+            self.free[self.lane_of[si]].append(si)
         self.inflight = still
         return done_any
 
@@ -199,7 +226,7 @@ class PersistentServer:
         return a or b
 
     def idle(self) -> bool:
-        return not self.queue and not self.inflight
+        return not self.queues[0] and not self.queues[1] and not self.inflight
 
     def serve(self, requests: Sequence, arrivals: Sequence[float],
               clock: Callable[[], float] = time.perf_counter) -> List[Job]:
