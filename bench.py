@@ -94,6 +94,10 @@ def parse(argv=None):
     ap.add_argument("--profile-case", action="store_true",
                     help="only run the small profiling case (one persistent launch of 8 "
                          "requests, twice) and print its per-request device times")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="with --profile-case: mixed precision (3xTF32 tensor-core products "
+                         "inside float64 refinement) and iterative local solves above 50 "
+                         "unknowns")
     return ap.parse_args(argv)
 
 
@@ -490,10 +494,12 @@ def rounding_run(torch, pairs=1024, reps=5):
             "precision": "float64 (no 3xTF32 rounding variant)"}
 
 
-def profile_case():
+def profile_case(mixed: bool = False):
     """The small case profiled with ncu: one persistent launch of 8 requests
     (2-D QTT Poisson with 8, 12, 16, 20 cores; diffusion d = 4, 6 with
-    n = 16, 32), run twice (the second launch is the captured one)."""
+    n = 16, 32), run twice (the second launch is the captured one).  With
+    ``mixed`` the local solves above 50 unknowns are iterative and run in
+    mixed precision."""
     import torch
 
     from ttnumpy_b200 import problems as P
@@ -502,6 +508,8 @@ def profile_case():
     torch.cuda.set_device(0)
     kw = dict(residual_tol=TOL, symmetric=True, max_sweeps=MAX_SWEEPS, seed=0,
               stagnation_factor=None)
+    if mixed:
+        kw.update(precision="mixed", direct_solve_size=50)
     rng = np.random.default_rng(11)
     reqs = []
     for N in (4, 6, 8, 10):
@@ -518,13 +526,14 @@ def profile_case():
     res = batch.collect()
     print(json.dumps({"status": [r.status for r in res],
                       "gflop": sum(r.flops for r in res) / 1e9,
+                      "gflop_tc": sum(r.flops_tc for r in res) / 1e9,
                       "device_ms": [round(r.device_ms, 1) for r in res]}))
 
 
 def main():
     args = parse()
     if args.profile_case:
-        profile_case()
+        profile_case(args.profile_mixed)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
