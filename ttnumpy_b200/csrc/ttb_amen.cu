@@ -164,104 +164,124 @@ struct VecArgs {
   i64 N;
 };
 
-// One chunk of a pass (pairs of doubles; the odd last element goes to the
-// last chunk); returns the chunk's sum, the same on every thread.
+// The pairs lo .. hi of a pass (and, with ``tail``, the odd last element);
+// returns this thread's partial sum (its pairs in index order, then the
+// tail).  Each thread loads kVecBatch pairs of every input before it stores
+// any output, so that those loads are in flight together (a store may alias
+// a later load, which keeps the compiler from reordering them itself).
 //   VP_SCALE:   p0 = a0 p1                         (v = r2 / beta)
 //   VP_LANCZOS: p0 -= a0 p1 unless first; sum p2 . p0   (y, r1, v)
 //   VP_RESID:   p0 = p1 - a0 p2; sum p0 . p0        (r1 <- y - g r2)
 //   VP_UPDATE:  p0 <- (p2 - a0 p0 - a1 p1) a2; p3 += a3 p0; sum p3 . p3
 //               (w2 <- new w from v, w2, w; x += phi w)
+constexpr int kVecBatch = 4;
+
+template <int OP>
+__device__ __forceinline__ double vpass_range(const VecArgs& q, i64 lo, i64 hi, bool tail) {
+  double acc = 0.0;
+  double2* P0 = reinterpret_cast<double2*>(q.p0);
+  const double2* P1 = reinterpret_cast<const double2*>(q.p1);
+  const double2* P2 = reinterpret_cast<const double2*>(q.p2);
+  double2* P3 = reinterpret_cast<double2*>(q.p3);
+  const bool upd = OP != VP_LANCZOS || !q.first;
+  for (i64 i0 = lo + threadIdx.x; i0 < hi; i0 += kVecBatch * TTB_THREADS) {
+    double2 u0[kVecBatch], u1[kVecBatch], u2[kVecBatch], u3[kVecBatch];
+#pragma unroll
+    for (int b = 0; b < kVecBatch; ++b) {
+      const i64 i = i0 + (i64)b * TTB_THREADS;
+      if (i >= hi) break;
+      if (OP == VP_SCALE) {
+        u1[b] = P1[i];
+      } else if (OP == VP_LANCZOS) {
+        u0[b] = P0[i];
+        u2[b] = P2[i];
+        if (upd) u1[b] = P1[i];
+      } else if (OP == VP_RESID) {
+        u1[b] = P1[i];
+        u2[b] = P2[i];
+      } else {
+        u0[b] = P0[i];
+        u1[b] = P1[i];
+        u2[b] = P2[i];
+        u3[b] = P3[i];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kVecBatch; ++b) {
+      const i64 i = i0 + (i64)b * TTB_THREADS;
+      if (i >= hi) break;
+      if (OP == VP_SCALE) {
+        P0[i] = make_double2(q.a0 * u1[b].x, q.a0 * u1[b].y);
+      } else if (OP == VP_LANCZOS) {
+        double2 yy = u0[b];
+        const double2 vv = u2[b];
+        if (upd) {
+          const double2 rr = u1[b];
+          yy.x -= q.a0 * rr.x;
+          yy.y -= q.a0 * rr.y;
+          P0[i] = yy;
+        }
+        acc = fma(vv.x, yy.x, acc);
+        acc = fma(vv.y, yy.y, acc);
+      } else if (OP == VP_RESID) {
+        const double2 yy = u1[b], rr = u2[b];
+        const double2 nv = make_double2(yy.x - q.a0 * rr.x, yy.y - q.a0 * rr.y);
+        P0[i] = nv;
+        acc = fma(nv.x, nv.x, acc);
+        acc = fma(nv.y, nv.y, acc);
+      } else {
+        const double2 a1 = u0[b], a2 = u1[b], vv = u2[b];
+        double2 xx = u3[b];
+        const double2 wn = make_double2((vv.x - q.a0 * a1.x - q.a1 * a2.x) * q.a2,
+                                        (vv.y - q.a0 * a1.y - q.a1 * a2.y) * q.a2);
+        P0[i] = wn;
+        xx.x += q.a3 * wn.x;
+        xx.y += q.a3 * wn.y;
+        P3[i] = xx;
+        acc = fma(xx.x, xx.x, acc);
+        acc = fma(xx.y, xx.y, acc);
+      }
+    }
+  }
+  if (tail) {
+    const i64 t = q.N - 1;
+    if (OP == VP_SCALE) {
+      q.p0[t] = q.a0 * q.p1[t];
+    } else if (OP == VP_LANCZOS) {
+      double yi = q.p0[t];
+      if (upd) {
+        yi -= q.a0 * q.p1[t];
+        q.p0[t] = yi;
+      }
+      acc = fma(q.p2[t], yi, acc);
+    } else if (OP == VP_RESID) {
+      const double yi = q.p1[t] - q.a0 * q.p2[t];
+      q.p0[t] = yi;
+      acc = fma(yi, yi, acc);
+    } else {
+      const double wn = (q.p2[t] - q.a0 * q.p0[t] - q.a1 * q.p1[t]) * q.a2;
+      q.p0[t] = wn;
+      const double xi = q.p3[t] + q.a3 * wn;
+      q.p3[t] = xi;
+      acc = fma(xi, xi, acc);
+    }
+  }
+  return acc;
+}
+
+// One chunk of a pass (pairs of doubles; the odd last element goes to the
+// last chunk); returns the chunk's sum, the same on every thread.
 __device__ __noinline__ double vpass_chunk(const VecArgs& q, int chunk, double* red) {
   const i64 N2 = q.N >> 1;
   const i64 cs = (N2 + kVecChunks - 1) / kVecChunks;
   const i64 lo = min((i64)chunk * cs, N2), hi = min(lo + cs, N2);
   const bool tail = (q.N & 1) && chunk == kVecChunks - 1 && threadIdx.x == 0;
-  double acc = 0.0;
+  double acc;
   switch (q.op) {
-    case VP_SCALE: {
-      const double2* R = reinterpret_cast<const double2*>(q.p1);
-      double2* V = reinterpret_cast<double2*>(q.p0);
-#pragma unroll 4
-      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
-        const double2 a = R[i];
-        V[i] = make_double2(q.a0 * a.x, q.a0 * a.y);
-      }
-      if (tail) q.p0[q.N - 1] = q.a0 * q.p1[q.N - 1];
-      break;
-    }
-    case VP_LANCZOS: {
-      double2* Y = reinterpret_cast<double2*>(q.p0);
-      const double2* R1 = reinterpret_cast<const double2*>(q.p1);
-      const double2* V = reinterpret_cast<const double2*>(q.p2);
-#pragma unroll 4
-      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
-        double2 yy = Y[i];
-        const double2 vv = V[i];
-        if (!q.first) {
-          const double2 rr = R1[i];
-          yy.x -= q.a0 * rr.x;
-          yy.y -= q.a0 * rr.y;
-          Y[i] = yy;
-        }
-        acc = fma(vv.x, yy.x, acc);
-        acc = fma(vv.y, yy.y, acc);
-      }
-      if (tail) {
-        double yi = q.p0[q.N - 1];
-        if (!q.first) {
-          yi -= q.a0 * q.p1[q.N - 1];
-          q.p0[q.N - 1] = yi;
-        }
-        acc = fma(q.p2[q.N - 1], yi, acc);
-      }
-      break;
-    }
-    case VP_RESID: {
-      double2* O = reinterpret_cast<double2*>(q.p0);
-      const double2* Y = reinterpret_cast<const double2*>(q.p1);
-      const double2* R2 = reinterpret_cast<const double2*>(q.p2);
-#pragma unroll 4
-      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
-        const double2 yy = Y[i], rr = R2[i];
-        const double2 nv = make_double2(yy.x - q.a0 * rr.x, yy.y - q.a0 * rr.y);
-        O[i] = nv;
-        acc = fma(nv.x, nv.x, acc);
-        acc = fma(nv.y, nv.y, acc);
-      }
-      if (tail) {
-        const double yi = q.p1[q.N - 1] - q.a0 * q.p2[q.N - 1];
-        q.p0[q.N - 1] = yi;
-        acc = fma(yi, yi, acc);
-      }
-      break;
-    }
-    default: {
-      double2* W2 = reinterpret_cast<double2*>(q.p0);
-      const double2* W = reinterpret_cast<const double2*>(q.p1);
-      const double2* V = reinterpret_cast<const double2*>(q.p2);
-      double2* X = reinterpret_cast<double2*>(q.p3);
-#pragma unroll 4
-      for (i64 i = lo + threadIdx.x; i < hi; i += TTB_THREADS) {
-        const double2 a1 = W2[i], a2 = W[i], vv = V[i];
-        double2 xx = X[i];
-        const double2 wn = make_double2((vv.x - q.a0 * a1.x - q.a1 * a2.x) * q.a2,
-                                        (vv.y - q.a0 * a1.y - q.a1 * a2.y) * q.a2);
-        W2[i] = wn;
-        xx.x += q.a3 * wn.x;
-        xx.y += q.a3 * wn.y;
-        X[i] = xx;
-        acc = fma(xx.x, xx.x, acc);
-        acc = fma(xx.y, xx.y, acc);
-      }
-      if (tail) {
-        const double wn = (q.p2[q.N - 1] - q.a0 * q.p0[q.N - 1] - q.a1 * q.p1[q.N - 1]) * q.a2;
-        q.p0[q.N - 1] = wn;
-        const double xi = q.p3[q.N - 1] + q.a3 * wn;
-        q.p3[q.N - 1] = xi;
-        acc = fma(xi, xi, acc);
-      }
-      break;
-    }
+    case VP_SCALE: acc = vpass_range<VP_SCALE>(q, lo, hi, tail); break;
+    case VP_LANCZOS: acc = vpass_range<VP_LANCZOS>(q, lo, hi, tail); break;
+    case VP_RESID: acc = vpass_range<VP_RESID>(q, lo, hi, tail); break;
+    default: acc = vpass_range<VP_UPDATE>(q, lo, hi, tail); break;
   }
   return block_sum(acc, red);
 }
@@ -372,6 +392,7 @@ struct SpOp {
   const double* val;
   int rows;  // 0: no sparse form (the dense product is used)
   int nnz;
+  int cols;  // columns of the sparse form (rows of the dense operand)
 };
 
 // Cores below this many entries, or denser than one nonzero in kSpDensity,
@@ -441,6 +462,7 @@ __device__ __noinline__ SpOp build_spop(Ctx& c, const double* op, int R, int n, 
   S.val = val;
   S.rows = rows;
   S.nnz = nnz;
+  S.cols = cols;
   return S;
 }
 
@@ -471,6 +493,102 @@ __device__ __noinline__ void spmm_rows(const int* ptr, const int* col, const dou
   __syncthreads();
 }
 
+// The lone block's product for an operand with unit column stride, staged
+// through the shared pool: the sparse form (row starts, columns, values) is
+// copied in once, then column tiles of B (all S.cols rows, 64 U columns)
+// are copied in with cp.async and worked on from shared memory.  A warp
+// takes one row at a time and walks its terms; each lane owns U pairs of
+// adjacent columns (16-byte shared loads), so the term's value and column
+// are loaded once for 2 U outputs.  Every output element sums its row's
+// terms in column order, as spmm_rows does from global memory (the same
+// bits).  Without the staging each term is a chain of dependent global
+// loads (column index, then operand), which left the product bound by load
+// latency.  The pool is free whenever a product runs: only the
+// factorisations, the direct solves and the tensor-core stages use it, each
+// within its own call.
+__device__ __forceinline__ int spmm_tile(const SpOp& S) {
+  const i64 meta = S.nnz + (S.nnz + 1) / 2 + (S.rows + 2) / 2;
+  if (S.cols <= 0 || meta >= kPoolD) return 0;
+  const i64 tw = (kPoolD - meta) / S.cols;
+  return tw >= 128 ? 128 : tw >= 64 ? 64 : 0;
+}
+
+template <int U>
+__device__ __forceinline__ void spmm_tile_rows(const double* tile, const double* val,
+                                               const int* col, const int* ptr, int rows, int j0,
+                                               int w, const OMat& C, double alpha, double beta) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  i64 coff[U][2];
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int jj = 64 * u + 2 * lane + h;
+      coff[u][h] = jj < w ? C.col(j0 + jj) : 0;
+    }
+  for (int r = warp; r < rows; r += TTB_WARPS) {
+    const int e0 = ptr[r], e1 = ptr[r + 1];
+    double2 acc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc[u] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int e = e0; e < e1; ++e) {
+      const double v = val[e];
+      const double* trow = tile + col[e] + 2 * lane;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        // columns at and beyond w hold stale values; their sums are dropped
+        const double2 b = *reinterpret_cast<const double2*>(trow + 64 * u);
+        acc[u].x = fma(v, b.x, acc[u].x);
+        acc[u].y = fma(v, b.y, acc[u].y);
+      }
+    }
+    double* crow = C.p + C.row(r);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (64 * u + 2 * lane + h >= w) continue;
+        double* cp = crow + coff[u][h];
+        double v = alpha * (h ? acc[u].y : acc[u].x);
+        if (beta != 0.0) v = fma(beta, *cp, v);
+        *cp = v;
+      }
+  }
+}
+
+__device__ __noinline__ void spmm_staged(Ctx& c, const SpOp& S, const double* B, i64 b_rs, OMat C,
+                                         int N, double alpha, double beta, int tw) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rows = S.rows, cols = S.cols, nnz = S.nnz;
+  double* tile = c.pool;  // cols x tw, rows 16-byte aligned
+  double* val = tile + (i64)cols * tw;
+  int* col = reinterpret_cast<int*>(val + nnz);
+  int* ptr = reinterpret_cast<int*>(val + nnz + (nnz + 1) / 2);
+  __syncthreads();  // the pool's previous user is done with it
+  for (int e = threadIdx.x; e < nnz; e += TTB_THREADS) {
+    val[e] = S.val[e];
+    col[e] = S.col[e] * tw;
+  }
+  for (int r = threadIdx.x; r <= rows; r += TTB_THREADS) ptr[r] = S.ptr[r];
+  for (int j0 = 0; j0 < N; j0 += tw) {
+    const int w = min(tw, N - j0);
+    for (int q = warp; q < cols; q += TTB_WARPS) {
+      const double* src = B + (i64)q * b_rs + j0;
+      double* dst = tile + (i64)q * tw;
+      for (int jj = lane; jj < w; jj += 32) cp_async8(dst + jj, src + jj, true);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();  // the tile (and the sparse form) landed
+    if (tw == 128)
+      spmm_tile_rows<2>(tile, val, col, ptr, rows, j0, w, C, alpha, beta);
+    else
+      spmm_tile_rows<1>(tile, val, col, ptr, rows, j0, w, C, alpha, beta);
+    __syncthreads();  // the tile's reads are done before the next copy
+  }
+}
+
 __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_rs, i64 b_cs,
                                   OMat C, int N, double alpha, double beta) {
   c.flops += 2.0 * S.nnz * (double)N;
@@ -495,6 +613,14 @@ __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_
     cluster_barrier();
     spmm_rows(S.ptr, S.col, S.val, S.rows, B, b_rs, b_cs, C, N, alpha, beta, 0, c.csize);
     cluster_barrier();
+    c.cyc[PH_GEMM] += clock64() - t0;
+    return;
+  }
+  const int tw = (b_cs == 1 && !__isShared(B) && !__isShared(C.p) && !__isShared(S.val))
+                     ? spmm_tile(S)
+                     : 0;
+  if (tw > 0) {
+    spmm_staged(c, S, B, b_rs, C, N, alpha, beta, tw);
     c.cyc[PH_GEMM] += clock64() - t0;
     return;
   }
@@ -967,77 +1093,24 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
   int istop = 0;
   for (int itn = 1; itn <= maxit; ++itn) {
     const double s = 1.0 / beta;
-    if (chunked) {
+    if (chunked)
       vpass(c, VecArgs{VP_SCALE, 0, s, 0.0, 0.0, 0.0, v, r2, nullptr, nullptr, N});
-    } else {
-      const double2* R2 = reinterpret_cast<const double2*>(r2);
-      double2* V = reinterpret_cast<double2*>(v);
-#pragma unroll 4
-      for (i64 i = threadIdx.x; i < N2; i += TTB_THREADS) {
-        const double2 a = R2[i];
-        V[i] = make_double2(s * a.x, s * a.y);
-      }
-      if (tail) v[N - 1] = s * r2[N - 1];
-    }
+    else
+      vpass_range<VP_SCALE>(VecArgs{VP_SCALE, 0, s, 0.0, 0.0, 0.0, v, r2, nullptr, nullptr, N}, 0,
+                            N2, tail);
     __syncthreads();
     apply(c, L, v, y, 1, 1.0, 0.0, tc);
     if (c.status) return;
     // y -= (beta / oldb) r1 and alfa = v . y in one pass
-    double dot = 0.0, alfa;
-    if (chunked) {
-      alfa = vpass(c, VecArgs{VP_LANCZOS, itn == 1, itn >= 2 ? beta / oldb : 0.0, 0.0, 0.0, 0.0,
-                              y, r1, v, nullptr, N});
-    } else {
-      const double f = itn >= 2 ? beta / oldb : 0.0;
-      const double2* V = reinterpret_cast<const double2*>(v);
-      const double2* R1 = reinterpret_cast<const double2*>(r1);
-      double2* Y = reinterpret_cast<double2*>(y);
-#pragma unroll 4
-      for (i64 i = threadIdx.x; i < N2; i += TTB_THREADS) {
-        double2 yy = Y[i];
-        const double2 vv = V[i];
-        if (itn >= 2) {
-          const double2 rr = R1[i];
-          yy.x -= f * rr.x;
-          yy.y -= f * rr.y;
-          Y[i] = yy;
-        }
-        dot = fma(vv.x, yy.x, dot);
-        dot = fma(vv.y, yy.y, dot);
-      }
-      if (tail) {
-        double yi = y[N - 1];
-        if (itn >= 2) {
-          yi -= f * r1[N - 1];
-          y[N - 1] = yi;
-        }
-        dot = fma(v[N - 1], yi, dot);
-      }
-      alfa = block_sum(dot, red);
-    }
+    const VecArgs lz{VP_LANCZOS, itn == 1, itn >= 2 ? beta / oldb : 0.0, 0.0, 0.0, 0.0,
+                     y, r1, v, nullptr, N};
+    const double alfa =
+        chunked ? vpass(c, lz) : block_sum(vpass_range<VP_LANCZOS>(lz, 0, N2, tail), red);
     const double g = alfa / beta;
-    double part = 0.0, psum;
-    if (chunked) {
-      psum = vpass(c, VecArgs{VP_RESID, 0, g, 0.0, 0.0, 0.0, r1, y, r2, nullptr, N});
-    } else {
-      const double2* Y = reinterpret_cast<const double2*>(y);
-      const double2* R2 = reinterpret_cast<const double2*>(r2);
-      double2* R1 = reinterpret_cast<double2*>(r1);
-#pragma unroll 4
-      for (i64 i = threadIdx.x; i < N2; i += TTB_THREADS) {
-        const double2 yy = Y[i], rr = R2[i];
-        const double2 nv = make_double2(yy.x - g * rr.x, yy.y - g * rr.y);
-        R1[i] = nv;  // the new r2; r1 was last read above
-        part = fma(nv.x, nv.x, part);
-        part = fma(nv.y, nv.y, part);
-      }
-      if (tail) {
-        const double yi = y[N - 1] - g * r2[N - 1];
-        r1[N - 1] = yi;
-        part = fma(yi, yi, part);
-      }
-      psum = block_sum(part, red);
-    }
+    // r1 <- y - g r2 (the new r2) and its squared norm
+    const VecArgs rs{VP_RESID, 0, g, 0.0, 0.0, 0.0, r1, y, r2, nullptr, N};
+    const double psum =
+        chunked ? vpass(c, rs) : block_sum(vpass_range<VP_RESID>(rs, 0, N2, tail), red);
     {
       double* t = r1;
       r1 = r2;
@@ -1059,36 +1132,10 @@ __device__ __noinline__ void minres(Ctx& c, const LocalOp& L, const double* b, d
     const double phi = cs * phibar;
     phibar = sn * phibar;
     const double denom = 1.0 / gamma;
-    double xs = 0.0, xsum;
-    if (chunked) {
-      xsum = vpass(c, VecArgs{VP_UPDATE, 0, oldeps, delta, denom, phi, w2, w, v, x, N});
-    } else {
-      const double2* V = reinterpret_cast<const double2*>(v);
-      const double2* W = reinterpret_cast<const double2*>(w);
-      double2* W2 = reinterpret_cast<double2*>(w2);
-      double2* X = reinterpret_cast<double2*>(x);
-#pragma unroll 4
-      for (i64 i = threadIdx.x; i < N2; i += TTB_THREADS) {
-        const double2 a1 = W2[i], a2 = W[i], vv = V[i];
-        double2 xx = X[i];
-        const double2 wn = make_double2((vv.x - oldeps * a1.x - delta * a2.x) * denom,
-                                        (vv.y - oldeps * a1.y - delta * a2.y) * denom);
-        W2[i] = wn;  // the new w; the old w becomes w2
-        xx.x += phi * wn.x;
-        xx.y += phi * wn.y;
-        X[i] = xx;
-        xs = fma(xx.x, xx.x, xs);
-        xs = fma(xx.y, xx.y, xs);
-      }
-      if (tail) {
-        const double wn = (v[N - 1] - oldeps * w2[N - 1] - delta * w[N - 1]) * denom;
-        w2[N - 1] = wn;
-        const double xi = x[N - 1] + phi * wn;
-        x[N - 1] = xi;
-        xs = fma(xi, xi, xs);
-      }
-      xsum = block_sum(xs, red);
-    }
+    // the new w (into w2's buffer) and x += phi w, with x's squared norm
+    const VecArgs up{VP_UPDATE, 0, oldeps, delta, denom, phi, w2, w, v, x, N};
+    const double xsum =
+        chunked ? vpass(c, up) : block_sum(vpass_range<VP_UPDATE>(up, 0, N2, tail), red);
     {
       double* t = w2;
       w2 = w;
