@@ -375,37 +375,30 @@ static __device__ __forceinline__ bool gemm_pipe_tiled(CMat A, CMat B, int M, in
   return true;
 }
 
-// ``tile0`` and ``tstride``: on the tiled path, compute only the output
-// tiles tile0, tile0 + tstride, ... (row-major tile order), each exactly as
-// the whole product computes it.
-static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
+// The tiled path of cta_gemm_pipe for TM x TN output tiles (eight warps of
+// 32 x 16, TN / 16 of them along N), K staged TK at a time through an
+// NS-stage cp.async ring.  Each output element accumulates its K range in
+// steps of four (one DMMA each) in increasing order whatever the tile
+// shape, so every shape gives the same bits.
+template <int TM, int TN, int TK, int NS>
+static __device__ __forceinline__ void gemm_tiles(CMat A, CMat B, OMat C, int M, int N, int K,
                                                   double alpha, double beta, double* ring,
-                                                  int tile0 = 0, int tstride = 1) {
-  if (M <= 0 || N <= 0) return;
-  // cp.async copies from global memory only: operands in shared memory, and
-  // K == 0 (C = beta * C), go through the one-stage tile
-  if (K <= 0 || __isShared(A.p) || __isShared(B.p)) {
-    cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
-    return;
-  }
-  // (operands contiguous along K only: the split-K loads read 32-byte runs of K)
-  if (K >= kSkinnyK && A.cs == 1 && B.rs == 1) {
-    if (M <= 16 && N <= 48) {
-      cta_gemm_skinny<2, 6>(A, B, C, M, N, K, alpha, beta, ring);
-      return;
-    }
-    if (M <= 48 && N <= 16) {
-      cta_gemm_skinny<6, 2>(A, B, C, M, N, K, alpha, beta, ring);
-      return;
-    }
-  }
+                                                  int tile0, int tstride) {
+  static_assert(TTB_WARPS == 8 && TM * TN == 8 * 32 * 16, "eight warps of 32 x 16");
+  static_assert(TK % 4 == 0, "K steps of four");
+  constexpr int PA = TM + 4, PB = TN + 4;  // pitches: see GPITCH_A
+  constexpr int SD = TK * (PA + PB);       // doubles of a stage
+  static_assert(NS * SD <= GSTAGES * GSTAGE_D, "stages must fit the ring");
+  constexpr int NA = (TM * TK) / TTB_THREADS;
+  constexpr int NB = (TK * TN + TTB_THREADS - 1) / TTB_THREADS;
+  static_assert(NA * TTB_THREADS == TM * TK, "A tile loads must divide evenly");
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+  const int wm = (warp / (TN / 16)) * 32, wn = (warp % (TN / 16)) * 16;
   const int g = lane >> 2, t = lane & 3;
-  const int tn = (N + GBN - 1) / GBN;
-  const int nk = (K + GBK - 1) / GBK;
-  const int tiles = ((M + GBM - 1) / GBM) * tn;
+  const int tn = (N + TN - 1) / TN;
+  const int nk = (K + TK - 1) / TK;
+  const int tiles = ((M + TM - 1) / TM) * tn;
   const int nloc = tile0 < tiles ? (tiles - tile0 + tstride - 1) / tstride : 0;
   const int total = nloc * nk;
   const bool a_kfast = (A.cs == 1);
@@ -413,33 +406,33 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
   auto issue = [&](int step) {
     if (step < total) {
       const int tile = tile0 + (step / nk) * tstride, kt = step % nk;
-      const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN, k0 = kt * GBK;
-      double* sa = ring + (step % GSTAGES) * GSTAGE_D;
-      double* sb = sa + GBK * GPITCH_A;
+      const int m0 = (tile / tn) * TM, n0 = (tile % tn) * TN, k0 = kt * TK;
+      double* sa = ring + (step % NS) * SD;
+      double* sb = sa + TK * PA;
 #pragma unroll
-      for (int e = 0; e < GNA; ++e) {
+      for (int e = 0; e < NA; ++e) {
         const int idx = tid + e * TTB_THREADS;
         int mm, kk;
-        if (a_kfast) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
+        if (a_kfast) { kk = idx % TK; mm = idx / TK; } else { mm = idx % TM; kk = idx / TM; }
         const int gm = m0 + mm, gk = k0 + kk;
         const bool oka = gm < M && gk < K;
-        cp_async8(sa + kk * GPITCH_A + mm, oka ? A.p + gm * A.rs + gk * A.cs : A.p, oka);
+        cp_async8(sa + kk * PA + mm, oka ? A.p + gm * A.rs + gk * A.cs : A.p, oka);
       }
 #pragma unroll
-      for (int e = 0; e < GNB; ++e) {
+      for (int e = 0; e < NB; ++e) {
         const int idx = tid + e * TTB_THREADS;
-        if (idx >= GBK * GBN) break;
+        if (idx >= TK * TN) break;
         int nn, kb;
-        if (b_nfast) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
+        if (b_nfast) { nn = idx % TN; kb = idx / TN; } else { kb = idx % TK; nn = idx / TK; }
         const int gn = n0 + nn, gk2 = k0 + kb;
         const bool okb = gn < N && gk2 < K;
-        cp_async8(sb + kb * GPITCH_B + nn, okb ? B.p + gk2 * B.rs + gn * B.cs : B.p, okb);
+        cp_async8(sb + kb * PB + nn, okb ? B.p + gk2 * B.rs + gn * B.cs : B.p, okb);
       }
     }
     cp_async_commit();
   };
 #pragma unroll
-  for (int st = 0; st < GSTAGES - 1; ++st) issue(st);
+  for (int st = 0; st < NS - 1; ++st) issue(st);
   double acc[4][2][2];
   for (int step = 0; step < total; ++step) {
     const int kt = step % nk;
@@ -449,18 +442,18 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
 #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     }
-    cp_async_wait_ahead();
+    asm volatile("cp.async.wait_group %0;" ::"n"(NS - 2) : "memory");
     __syncthreads();  // this step's operands landed; the previous step's reads are done
-    issue(step + GSTAGES - 1);
-    const double* sa = ring + (step % GSTAGES) * GSTAGE_D;
-    const double* sb = sa + GBK * GPITCH_A;
+    issue(step + NS - 1);
+    const double* sa = ring + (step % NS) * SD;
+    const double* sb = sa + TK * PA;
 #pragma unroll
-    for (int kk = 0; kk < GBK; kk += 4) {
+    for (int kk = 0; kk < TK; kk += 4) {
       double av[4], bv[2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * GPITCH_A + wm + 8 * i + g];
+      for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * PA + wm + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) bv[j] = sb[(kk + t) * GPITCH_B + wn + 8 * j + g];
+      for (int j = 0; j < 2; ++j) bv[j] = sb[(kk + t) * PB + wn + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -468,7 +461,7 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
     }
     if (kt == nk - 1) {
       const int tile = tile0 + (step / nk) * tstride;
-      const int m0 = (tile / tn) * GBM, n0 = (tile % tn) * GBN;
+      const int m0 = (tile / tn) * TM, n0 = (tile % tn) * TN;
       i64 coff[2][2];
 #pragma unroll
       for (int j = 0; j < 2; ++j)
@@ -493,6 +486,39 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
     }
   }
   cp_async_wait_all();
+}
+
+
+// ``tile0`` and ``tstride``: on the tiled path, compute only the output
+// tiles tile0, tile0 + tstride, ... (row-major tile order), each exactly as
+// the whole product computes it.
+static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M, int N, int K,
+                                                  double alpha, double beta, double* ring,
+                                                  int tile0 = 0, int tstride = 1) {
+  if (M <= 0 || N <= 0) return;
+  // cp.async copies from global memory only: operands in shared memory, and
+  // K == 0 (C = beta * C), go through the one-stage tile
+  if (K <= 0 || __isShared(A.p) || __isShared(B.p)) {
+    cta_gemm(A, B, C, M, N, K, alpha, beta, *reinterpret_cast<GemmSmem*>(ring));
+    return;
+  }
+  // (operands contiguous along K only: the split-K loads read 32-byte runs of K)
+  if (K >= kSkinnyK && A.cs == 1 && B.rs == 1) {
+    if (M <= 16 && N <= 48) {
+      cta_gemm_skinny<2, 6>(A, B, C, M, N, K, alpha, beta, ring);
+      return;
+    }
+    if (M <= 48 && N <= 16) {
+      cta_gemm_skinny<6, 2>(A, B, C, M, N, K, alpha, beta, ring);
+      return;
+    }
+  }
+  // outputs of at most 32 columns: 128 x 32 tiles (a 64 x 64 tile would
+  // leave half or more of its columns empty)
+  if (N <= 32 && M > 64)
+    gemm_tiles<128, 32, 12, 3>(A, B, C, M, N, K, alpha, beta, ring, tile0, tstride);
+  else
+    gemm_tiles<GBM, GBN, GBK, GSTAGES>(A, B, C, M, N, K, alpha, beta, ring, tile0, tstride);
   __syncthreads();  // callers may reuse the ring and read C right away
 }
 
