@@ -447,8 +447,10 @@ static __device__ __forceinline__ void gemm_tiles(CMat A, CMat B, OMat C, int M,
     issue(step + NS - 1);
     const double* sa = ring + (step % NS) * SD;
     const double* sb = sa + TK * PA;
+    const int kvalid = K - kt * TK;  // the last slab's groups of four past K are zeros: skipped
 #pragma unroll
     for (int kk = 0; kk < TK; kk += 4) {
+      if (kk >= kvalid) break;
       double av[4], bv[2];
 #pragma unroll
       for (int i = 0; i < 4; ++i) av[i] = sa[(kk + t) * PA + wm + 8 * i + g];
