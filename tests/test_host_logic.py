@@ -96,3 +96,24 @@ def test_serving_mix_generator():
             assert len(p.A) == 24 and p.A[0].shape[1] == 64 and max(c.shape[0] for c in p.b) == 8
     arrivals = [t for t, _ in P.serving_stream(50, rate=10.0, seed=3)]
     assert all(t1 > t0 for t0, t1 in zip(arrivals, arrivals[1:]))
+
+
+def test_split_index_division_formula():
+    """The multiply-shift division the kernels use for split-index outputs
+    (FastDiv in csrc/ttb_device.cuh: m = floor(2^32 (2^l - d) / d) + 1 with
+    l = ceil(log2 d), n / d = (mulhi(m, n) + n) >> l for 0 <= n < 2^31),
+    restated here and checked against integer division."""
+    rng = np.random.default_rng(3)
+    divisors = list(range(1, 600)) + [int(v) for v in rng.integers(600, 1 << 30, 400)]
+    for d in divisors:
+        l = (d - 1).bit_length()
+        m = ((1 << 32) * ((1 << l) - d)) // d + 1
+        assert 0 < m < (1 << 32)
+        ns = [0, 1, d - 1, d, d + 1, 3 * d - 1, (1 << 31) - 1]
+        ns += [int(v) for v in rng.integers(0, 1 << 31, 50)]
+        for n in ns:
+            if n < 0 or n >= (1 << 31):
+                continue
+            t = ((m * n) >> 32) + n
+            assert t < (1 << 32)
+            assert t >> l == n // d, (n, d)

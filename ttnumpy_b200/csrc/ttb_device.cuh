@@ -133,19 +133,47 @@ static __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double
 // a result whose two index groups interleave in memory (a tensor
 // contraction's output permuted for the next contraction).
 constexpr int kNoSplit = 1 << 30;
+
+// Division of 0 <= n < 2^31 by an invariant d >= 1 as a multiply and a
+// shift (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, theorem 4.2 with N = 32): with l = ceil(log2 d)
+// and m = floor(2^32 (2^l - d) / d) + 1 (below 2^32),
+// n / d = (mulhi(m, n) + n) >> l, the sum staying below 2^32 for n < 2^31.
+// The split-index outputs divide every output index by their split sizes.
+struct FastDiv {
+  uint32_t m;
+  int l, d;
+  __device__ FastDiv() : m(1), l(0), d(1) {}
+  __device__ explicit FastDiv(int d_) : d(d_) {
+    l = 32 - __clz(d_ - 1);
+    m = (uint32_t)(((1ull << 32) * ((1ull << l) - (unsigned long long)d_)) / (unsigned)d_ + 1);
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi(m, (uint32_t)n) + (uint32_t)n) >> l);
+  }
+};
+
 struct OMat {
   double* p;
   i64 rs, cs, rs_hi, cs_hi;
   int rdiv, cdiv;
+  FastDiv rq, cq;  // rdiv and cdiv (when split)
   __device__ OMat(Mat m)
       : p(m.p), rs(m.rs), cs(m.cs), rs_hi(0), cs_hi(0), rdiv(kNoSplit), cdiv(kNoSplit) {}
   __device__ OMat(double* p_, int rdiv_, i64 rs_hi_, i64 rs_, int cdiv_, i64 cs_hi_, i64 cs_)
-      : p(p_), rs(rs_), cs(cs_), rs_hi(rs_hi_), cs_hi(cs_hi_), rdiv(rdiv_), cdiv(cdiv_) {}
+      : p(p_), rs(rs_), cs(cs_), rs_hi(rs_hi_), cs_hi(cs_hi_), rdiv(rdiv_), cdiv(cdiv_) {
+    if (rdiv != kNoSplit) rq = FastDiv(rdiv);
+    if (cdiv != kNoSplit) cq = FastDiv(cdiv);
+  }
   __device__ __forceinline__ i64 row(int i) const {
-    return rdiv == kNoSplit ? i * rs : (i / rdiv) * rs_hi + (i % rdiv) * rs;
+    if (rdiv == kNoSplit) return i * rs;
+    const int q = rq.div(i);
+    return q * rs_hi + (i - q * rdiv) * rs;
   }
   __device__ __forceinline__ i64 col(int j) const {
-    return cdiv == kNoSplit ? j * cs : (j / cdiv) * cs_hi + (j % cdiv) * cs;
+    if (cdiv == kNoSplit) return j * cs;
+    const int q = cq.div(j);
+    return q * cs_hi + (j - q * cdiv) * cs;
   }
 };
 
