@@ -301,7 +301,7 @@ struct ClusterCmd {
   const int* sp_ptr;
   const int* sp_col;
   const double* sp_val;
-  int sp_rows;
+  int sp_rows, sp_nnz, sp_cols;
 };
 
 __device__ __forceinline__ void cluster_barrier() {
@@ -493,8 +493,8 @@ __device__ __noinline__ void spmm_rows(const int* ptr, const int* col, const dou
   __syncthreads();
 }
 
-// The lone block's product for an operand with unit column stride, staged
-// through the shared pool: the sparse form (row starts, columns, values) is
+// The product for an operand with unit column stride, staged through the
+// block's shared pool: the sparse form (row starts, columns, values) is
 // copied in once, then column tiles of B (all S.cols rows, 64 U columns)
 // are copied in with cp.async and worked on from shared memory.  A warp
 // takes one row at a time and walks its terms; each lane owns U pairs of
@@ -505,11 +505,12 @@ __device__ __noinline__ void spmm_rows(const int* ptr, const int* col, const dou
 // loads (column index, then operand), which left the product bound by load
 // latency.  The pool is free whenever a product runs: only the
 // factorisations, the direct solves and the tensor-core stages use it, each
-// within its own call.
-__device__ __forceinline__ int spmm_tile(const SpOp& S) {
-  const i64 meta = S.nnz + (S.nnz + 1) / 2 + (S.rows + 2) / 2;
-  if (S.cols <= 0 || meta >= kPoolD) return 0;
-  const i64 tw = (kPoolD - meta) / S.cols;
+// within its own call (a cluster's other blocks use theirs for nothing
+// else).
+__device__ __forceinline__ int spmm_tile(int rows, int nnz, int cols) {
+  const i64 meta = nnz + (nnz + 1) / 2 + (rows + 2) / 2;
+  if (cols <= 0 || meta >= kPoolD) return 0;
+  const i64 tw = (kPoolD - meta) / cols;
   return tw >= 128 ? 128 : tw >= 64 ? 64 : 0;
 }
 
@@ -557,21 +558,24 @@ __device__ __forceinline__ void spmm_tile_rows(const double* tile, const double*
   }
 }
 
-__device__ __noinline__ void spmm_staged(Ctx& c, const SpOp& S, const double* B, i64 b_rs, OMat C,
-                                         int N, double alpha, double beta, int tw) {
+// The column tiles rank, rank + csize, ... of the staged product (each of a
+// cluster's blocks stages and computes its own tiles, all rows of each).
+__device__ __noinline__ void spmm_staged(double* pool, const int* sptr, const int* scol,
+                                         const double* sval, int rows, int nnz, int cols,
+                                         const double* B, i64 b_rs, OMat C, int N, double alpha,
+                                         double beta, int tw, int rank, int csize) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int rows = S.rows, cols = S.cols, nnz = S.nnz;
-  double* tile = c.pool;  // cols x tw, rows 16-byte aligned
+  double* tile = pool;  // cols x tw, rows 16-byte aligned
   double* val = tile + (i64)cols * tw;
   int* col = reinterpret_cast<int*>(val + nnz);
   int* ptr = reinterpret_cast<int*>(val + nnz + (nnz + 1) / 2);
   __syncthreads();  // the pool's previous user is done with it
   for (int e = threadIdx.x; e < nnz; e += TTB_THREADS) {
-    val[e] = S.val[e];
-    col[e] = S.col[e] * tw;
+    val[e] = sval[e];
+    col[e] = scol[e] * tw;
   }
-  for (int r = threadIdx.x; r <= rows; r += TTB_THREADS) ptr[r] = S.ptr[r];
-  for (int j0 = 0; j0 < N; j0 += tw) {
+  for (int r = threadIdx.x; r <= rows; r += TTB_THREADS) ptr[r] = sptr[r];
+  for (int j0 = rank * tw; j0 < N; j0 += csize * tw) {
     const int w = min(tw, N - j0);
     for (int q = warp; q < cols; q += TTB_WARPS) {
       const double* src = B + (i64)q * b_rs + j0;
@@ -587,6 +591,7 @@ __device__ __noinline__ void spmm_staged(Ctx& c, const SpOp& S, const double* B,
       spmm_tile_rows<1>(tile, val, col, ptr, rows, j0, w, C, alpha, beta);
     __syncthreads();  // the tile's reads are done before the next copy
   }
+  __syncthreads();  // (a block without tiles) the sparse form's copies are done
 }
 
 __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_rs, i64 b_cs,
@@ -602,6 +607,8 @@ __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_
       q.sp_col = S.col;
       q.sp_val = S.val;
       q.sp_rows = S.rows;
+      q.sp_nnz = S.nnz;
+      q.sp_cols = S.cols;
       q.b = B;
       q.b_rs = b_rs;
       q.b_cs = b_cs;
@@ -611,16 +618,22 @@ __device__ __noinline__ void spmm(Ctx& c, const SpOp& S, const double* B, i64 b_
       q.beta = beta;
     }
     cluster_barrier();
-    spmm_rows(S.ptr, S.col, S.val, S.rows, B, b_rs, b_cs, C, N, alpha, beta, 0, c.csize);
+    const int tw = b_cs == 1 ? spmm_tile(S.rows, S.nnz, S.cols) : 0;
+    if (tw > 0)
+      spmm_staged(c.pool, S.ptr, S.col, S.val, S.rows, S.nnz, S.cols, B, b_rs, C, N, alpha, beta,
+                  tw, 0, c.csize);
+    else
+      spmm_rows(S.ptr, S.col, S.val, S.rows, B, b_rs, b_cs, C, N, alpha, beta, 0, c.csize);
     cluster_barrier();
     c.cyc[PH_GEMM] += clock64() - t0;
     return;
   }
   const int tw = (b_cs == 1 && !__isShared(B) && !__isShared(C.p) && !__isShared(S.val))
-                     ? spmm_tile(S)
+                     ? spmm_tile(S.rows, S.nnz, S.cols)
                      : 0;
   if (tw > 0) {
-    spmm_staged(c, S, B, b_rs, C, N, alpha, beta, tw);
+    spmm_staged(c.pool, S.ptr, S.col, S.val, S.rows, S.nnz, S.cols, B, b_rs, C, N, alpha, beta,
+                tw, 0, 1);
     c.cyc[PH_GEMM] += clock64() - t0;
     return;
   }
@@ -2437,8 +2450,13 @@ __device__ __noinline__ void cluster_worker(Ctx& c, const ClusterCmd* lead, int 
         if (threadIdx.x == 0) c.vpart[k] = v;
       }
     } else {
-      spmm_rows(q.sp_ptr, q.sp_col, q.sp_val, q.sp_rows, q.b, q.b_rs, q.b_cs, cmd_out(q), q.N,
-                q.alpha, q.beta, rank, c.csize);
+      const int tw = q.b_cs == 1 ? spmm_tile(q.sp_rows, q.sp_nnz, q.sp_cols) : 0;
+      if (tw > 0)
+        spmm_staged(c.pool, q.sp_ptr, q.sp_col, q.sp_val, q.sp_rows, q.sp_nnz, q.sp_cols, q.b,
+                    q.b_rs, cmd_out(q), q.N, q.alpha, q.beta, tw, rank, c.csize);
+      else
+        spmm_rows(q.sp_ptr, q.sp_col, q.sp_val, q.sp_rows, q.b, q.b_rs, q.b_cs, cmd_out(q), q.N,
+                  q.alpha, q.beta, rank, c.csize);
     }
     cluster_barrier();  // this block's share is written
   }
