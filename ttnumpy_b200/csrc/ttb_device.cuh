@@ -543,9 +543,13 @@ static __device__ __noinline__ void cta_gemm_pipe(CMat A, CMat B, OMat C, int M,
       return;
     }
   }
-  // outputs of at most 32 columns: 128 x 32 tiles (a 64 x 64 tile would
-  // leave half or more of its columns empty)
-  if (N <= 32 && M > 64)
+  // 128 x 32 tiles where they cover the output with at least a fifth less
+  // padded area than 64 x 64 tiles (N <= 32 with M > 64, or N just above a
+  // multiple of 64, as 65-96): their operand loads per MMA are a fifth
+  // higher, so a smaller saving would not pay
+  const i64 pad64 = (i64)((M + 63) / 64 * 64) * ((N + 63) / 64 * 64);
+  const i64 pad128 = (i64)((M + 127) / 128 * 128) * ((N + 31) / 32 * 32);
+  if (5 * pad128 <= 4 * pad64)
     gemm_tiles<128, 32, 12, 3>(A, B, C, M, N, K, alpha, beta, ring, tile0, tstride);
   else
     gemm_tiles<GBM, GBN, GBK, GSTAGES>(A, B, C, M, N, K, alpha, beta, ring, tile0, tstride);
