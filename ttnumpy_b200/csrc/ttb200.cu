@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(TTB_THREADS) k_minres_a(const __grid_constant_
     const double ynorm = sqrt(sum_parts(q.part, q.chunks, 3));
     const int istop = minres_test(st, ynorm, q.rtol, q.maxit);
     if (istop != 0) {
-      // every block of the system computes the same verdict from the same
+      // every block of the system reaches the same stopping decision from the same
       // partial sums; block 0 records it
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (q.istop) *q.istop = istop;
